@@ -1,0 +1,319 @@
+"""Benchmark of the fused Euler step on B200.
+
+Workload (the headline configuration): 2D Kelvin-Helmholtz, 2048^2 interior
+cells, periodic, WENO5-Z + HLLC, SSPRK3, CFL 0.4, FP64, seeded synthetic
+initial conditions. One bench step = one full SSPRK3 step of the grid
+(3 fused stage kernels + a one-thread clock kernel), driven on the device
+(mc_advance: dt, the clock and the output clamp never leave the GPU).
+
+Prints one JSON line (rank 0). Metric: zone-updates/s = interior cells x
+steps / time. With --gpus N (one process per GPU under torchrun) every rank
+advances its own 2048^2 problem (independent problems, weak scaling); the
+timed region is bracketed by a barrier and device synchronisation and the
+time is the maximum over ranks.
+
+--impl reference times the reference's own CPU implementation of the same
+step (the reference's hot-path sources compiled against the host shim,
+oracle/_ref; the C restatement oracle/liboracle_port.so if that build is
+absent) with every host thread, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-updates/s"
+UNIT = "zone-updates/s"
+N_CELLS_SIDE = 2048
+WORKLOAD = "kelvin_helmholtz_2d_2048x2048_weno5z_hllc_ssprk3_fp64"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_CELLS_SIDE, help="cells per side (default 2048)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def config(n, precision, world):
+    return {"workload": WORKLOAD if (n == N_CELLS_SIDE and precision == "fp64") else
+            f"kelvin_helmholtz_2d_{n}x{n}_weno5z_hllc_ssprk3_{precision}",
+            "grid": f"{n}x{n}", "ghost_cells": 3, "vars": 4, "reconstruction": "weno5z",
+            "riemann_solver": "hllc", "time_stepper": "ssprk3", "cfl": 0.4, "gamma": 5.0 / 3.0,
+            "boundaries": "periodic", "per_rank_problem": f"one {n}x{n} problem per GPU",
+            "parallelism": f"independent problems x{world}",
+            "l2": "inputs larger than L2 (state 135 MB; each step streams ~400 MB), no flush"}
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic_per_launch():
+    """DRAM bytes per stage-kernel launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "stage2d_weno5z_hllc_kh2048_ncu.md")
+    try:
+        for ln in open(path):
+            if ln.startswith("traffic_bytes_per_launch:"):
+                return float(ln.split(":")[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference's own implementation
+# ---------------------------------------------------------------------------
+def cpu_oracle_kind():
+    from oracle import oracle as O
+    return "reference" if os.path.exists(O.LIB_PATHS["reference"]) else "port"
+
+
+def cpu_run(n, steps, warmup, budget_s=None):
+    """Time SSPRK3 steps of the KH problem on the host; returns (cells*steps/s, steps, seconds, kind, cores)."""
+    from oracle import oracle as O
+    from mosscap_b200 import problems as P
+    kind = cpu_oracle_kind()
+    cores = os.cpu_count() or 1
+    p = P.kelvin_helmholtz_2d(n, seed=0)
+    s = O.OracleSim(O.OracleConfig(**p.scheme_fields()), kind, threads=cores)
+    s.set_Q(p.Q)
+    s.fill_bcs()
+    for _ in range(warmup):
+        s.run(1)
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps:
+        s.run(1)
+        done += 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return n * n * done / dt, done, dt, kind, cores
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n = args.n
+    value, done, secs, kind, cores = cpu_run(n, args.steps, args.warmup)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * secs / done, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config(n, "fp64", 1),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": f"{done} full SSPRK3 steps of the {n}x{n} problem on {cores} threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU side
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from mosscap_b200 import problems as P
+    from mosscap_b200.hydro import HydroSim
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = args.n
+    p = P.kelvin_helmholtz_2d(n, seed=rank)
+    cells = n * n
+    sim = HydroSim(p, precision=args.precision, device=dev)
+    sim.fill_bcs()
+    if args.warmup:
+        sim.advance(args.warmup, log_dt=False)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # ---- timed region: K device-driven steps -----------------------------
+    phys = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+    gpu_index = int(phys[local]) if len(phys) > local and phys[local].strip().isdigit() else local
+    sampler = ClockSampler(gpu_index)
+    barrier()
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = sim.launch_count()
+    sim.profile_stages(True)
+    e0.record(stream)
+    steps_done = len(sim.advance(args.steps, log_dt=False)) if args.steps else 0
+    e1.record(stream)
+    barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    stage_ms, stage_n = sim.stage_time(0)
+    sim.profile_stages(False)
+    launches = sim.launch_count() - launches0
+    ms_max = max_over_ranks(ms)
+    assert steps_done == args.steps, "the device loop stopped early"
+    value = world * cells * args.steps / (ms_max / 1e3)
+    flags = sim.status()
+
+    # roofline of the dominant kernel (the fused stage kernel): algorithmic
+    # bytes per launch = the stage's state reads and writes, (3s-1) n_var 8 B
+    # per cell per step spread over s = 3 launches
+    nvar = 4
+    alg_bytes_per_launch = cells * (3 * 3 - 1) * nvar * 8 / 3.0
+    avg_launch_ms = stage_ms / max(stage_n, 1)
+    achieved = alg_bytes_per_launch / (avg_launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    traffic = ncu_traffic_per_launch()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": peak_kind, "kernel": "stage2d_kernel<WENO5Z,HLLC,f64>",
+                "alg_bytes_per_launch": alg_bytes_per_launch, "avg_launch_ms": avg_launch_ms,
+                "launches_timed": stage_n}
+
+    # ---- end to end through the C ABI with host buffers --------------------
+    e2e = None
+    if not args.no_e2e:
+        import ctypes
+        K = min(args.steps, 20) or 1
+        host = torch.empty(sim.Q.shape, dtype=torch.float64, pin_memory=True)
+        host.copy_(sim.Q)
+        qbytes = host.numel() * 8
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(K):
+            sim.Q.copy_(host, non_blocking=True)
+            dt = sim.compute_dt()          # dt back on the host, like the reference hook
+            sim.time_step(dt)
+            host.copy_(sim.Q, non_blocking=True)
+            torch.cuda.synchronize(dev)
+        barrier()
+        secs = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": world * cells * K / secs, "unit": UNIT, "h2d_bytes_per_step": qbytes,
+               "d2h_bytes_per_step": qbytes + 8,
+               "how": "per step: pinned-host state -> device, mc_compute_dt (dt read back), mc_time_step, "
+                      "state -> pinned host, synchronize"}
+
+    # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, done, secs, kind, cores = cpu_run(n, 1000, 1, budget_s=15.0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": f"{done} full SSPRK3 steps of the {n}x{n} problem ({secs:.1f} s, {cores} threads)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+                "data": "synthetic", "config": config(n, args.precision, world), "roofline": roofline,
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+                "status_flags": int(flags)}
+        print(json.dumps(line), flush=True)
+    del sim
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

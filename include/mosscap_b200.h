@@ -1,0 +1,206 @@
+/*
+ * mosscap_b200 -- C ABI of the B200 (sm_100a) finite-volume Euler step.
+ *
+ * The library replaces the hydro hooks that Mosscap installs on its
+ * Simulation aggregate (source/Simulation.hpp:38-62):
+ *   Simulation::time_step   void(Simulation&, fp_t dt)   -> mc_time_step
+ *   Simulation::compute_dt  f64(const Simulation&)       -> mc_compute_dt
+ *   fill_bcs(const Simulation&)                          -> mc_fill_bcs
+ * plus a device-resident driver of the main loop (source/main.cpp:54-72),
+ * mc_advance, which keeps dt, the clock and the output clamp on the GPU.
+ *
+ * Data contract (source/State.hpp:101-152): the conserved state Q is a
+ * caller-owned device array of doubles laid out [var][k][j][i] (i fastest)
+ * with ng ghost cells on both ends of every active axis; the variables are
+ * rho, m_x[, m_y[, m_z]], E followed by num_tracers passive mass densities.
+ * Q enters every step with its ghost cells filled (as the reference's
+ * time_step assumes) and leaves with them filled.
+ *
+ * Every call is exception-free and returns an mc_status. Calls are ordered
+ * on the stream they are given (a cudaStream_t passed as void*; NULL is the
+ * legacy default stream) and return without waiting, except where noted.
+ * One context must not be used from two threads at once.
+ */
+#ifndef MOSSCAP_B200_H
+#define MOSSCAP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MC_ABI_VERSION 1
+
+typedef enum {
+    MC_OK = 0,
+    MC_ERR_INVALID_ARGUMENT = 1, /* bad descriptor, null pointer, size out of range */
+    MC_ERR_UNSUPPORTED = 2,      /* combination the library does not implement */
+    MC_ERR_CUDA = 3,             /* a CUDA runtime call failed; see mc_last_error */
+    MC_ERR_OUT_OF_MEMORY = 4,
+    MC_ERR_STATE = 5             /* the device status word holds a physics flag */
+} mc_status;
+
+/* Physics flags accumulated on the device (mc_get_status). */
+#define MC_FLAG_NONFINITE 0x1u     /* a non-finite value in a state the step read or wrote */
+#define MC_FLAG_NEG_DENSITY 0x2u   /* rho <= 0 */
+#define MC_FLAG_NEG_PRESSURE 0x4u  /* p <= 0 */
+#define MC_FLAG_BAD_DT 0x8u        /* dt <= 0 or not finite */
+
+/* Enum values equal the reference's ordinals. */
+typedef enum { /* source/Reconstruct.hpp:10-15 */
+    MC_RECON_FOG = 0,
+    MC_RECON_MUSCL = 1,
+    MC_RECON_PPM = 2,
+    MC_RECON_WENO5Z = 3
+} mc_reconstruction;
+
+typedef enum { /* source/Reconstruct.hpp:22-26 */
+    MC_LIMITER_VANLEER = 0,
+    MC_LIMITER_MONOTONIZED_CENTRAL = 1,
+    MC_LIMITER_MINMOD = 2
+} mc_slope_limiter;
+
+typedef enum { /* source/Riemann.hpp:10-14 */
+    MC_RIEMANN_RUSANOV = 0,
+    MC_RIEMANN_HLL = 1,
+    MC_RIEMANN_HLLC = 2
+} mc_riemann_solver;
+
+typedef enum { /* source/TimeStepping.hpp:10-14 */
+    MC_STEPPER_RK2 = 0,
+    MC_STEPPER_SSPRK3 = 1,
+    MC_STEPPER_SSPRK4 = 2
+} mc_time_stepper;
+
+typedef enum { /* source/State.hpp:62-70 */
+    MC_BC_WALL = 0,
+    MC_BC_PERIODIC = 1,
+    MC_BC_SYMMETRIC = 2,
+    MC_BC_SYMMETRIC_OUTFLOW_DIODE = 3,
+    MC_BC_ZEROGRAD = 4,
+    MC_BC_CONSTANT = 5,
+    MC_BC_USERFN = 6 /* ghost cells left to the caller's hook after each fill */
+} mc_boundary_type;
+
+typedef enum {
+    /* Every operation in the reference's order without fused multiply-adds:
+     * bit-identical to the reference's CPU build. */
+    MC_PRECISION_FP64 = 0,
+    /* Reconstruction, Riemann fluxes and their EOS calls in FP32; the
+     * conserved state, the primitive recovery from it (pressure from total
+     * energy), the flux-divergence accumulation and dt stay FP64. */
+    MC_PRECISION_FP32_COMPENSATED = 1
+} mc_precision;
+
+/* Grid description; mirrors GridSize / State / Boundaries
+ * (source/State.hpp:72-152, set up as in source/SetupModules.hpp:9-136). */
+typedef struct {
+    int32_t num_dim;      /* 1, 2 or 3 */
+    int32_t xc, yc, zc;   /* cells per axis including ghosts; 1 on inactive axes */
+    int32_t ng;           /* ghost cells per side on active axes */
+    int32_t num_tracers;  /* passive scalars after the 2+num_dim hydro variables */
+    double dx;            /* cell width, equal on every axis */
+    double loc[3];        /* lower corner of the first interior cell (State::loc) */
+    int32_t bc[6];        /* xs, xe, ys, ye, zs, ze (mc_boundary_type) */
+    double bc_const[6][5];/* conserved values for MC_BC_CONSTANT faces, in variable order */
+} mc_grid;
+
+/* Numerical scheme; mirrors NumericalSchemes + Eos + max_cfl
+ * (source/Simulation.hpp:17-22, source/Eos.hpp:27-42). */
+typedef struct {
+    int32_t reconstruction; /* mc_reconstruction */
+    int32_t slope_limiter;  /* mc_slope_limiter (ignored by FOG and WENO5-Z) */
+    int32_t riemann_solver; /* mc_riemann_solver */
+    int32_t time_stepper;   /* mc_time_stepper */
+    int32_t precision;      /* mc_precision */
+    double gamma;           /* ideal-gas ratio of specific heats */
+    double max_cfl;         /* dt = max_cfl * min over cells of dx / (c_s + |v|) */
+} mc_scheme;
+
+/* Time bookkeeping of Simulation / OutputConfig (source/Simulation.hpp:40-44,
+ * source/Output.hpp:15-23): compute_dt clamps dt so that a step ends exactly
+ * on min(max_time, prev_output_time + output_delta) (source/Hydro.cpp:231-241). */
+typedef struct {
+    double time;
+    double max_time;
+    double prev_output_time;
+    double output_delta;
+} mc_clock;
+
+typedef struct mc_ctx mc_ctx;
+
+/* Create a context for one grid + scheme on the current CUDA device.
+ * Allocates the stage buffers (two states' worth) and a small device block.
+ * Rejects ng below the reconstruction's need (FOG 1, MUSCL 2, PPM / WENO5-Z 3;
+ * source/Reconstruct.hpp:47-61) and active axes with fewer than ng interior
+ * cells. Replaces Simulation setup (source/SetupModules.hpp:9-168). */
+mc_status mc_create(const mc_grid* grid, const mc_scheme* scheme, mc_ctx** out);
+mc_status mc_destroy(mc_ctx* ctx);
+
+/* Simulation::user_bc (source/Simulation.hpp:55, called at the end of
+ * fill_bcs, source/Boundaries.hpp:146-148): a host function that enqueues on
+ * `stream` the caller's own ghost fill of a state buffer. It is called after
+ * mc_fill_bcs and after every stage, with the stage's output buffer (which
+ * may be a library-owned buffer, not the caller's Q), and must be idempotent:
+ * mc_advance may call it for steps the device has already skipped. Required
+ * when any active face is MC_BC_USERFN. fn = NULL removes the hook. */
+mc_status mc_set_user_bc(mc_ctx* ctx, void (*fn)(void* user, double* Q, void* stream), void* user);
+
+/* fill_bcs (source/Boundaries.hpp:121-149): fill every ghost cell of Q from
+ * the interior for the built-in boundary kinds, x then y then z. */
+mc_status mc_fill_bcs(mc_ctx* ctx, double* Q, void* stream);
+
+/* compute_dt (source/Hydro.cpp:209-242): min over every cell, ghosts
+ * included, of dx / (c_s + |v|), times max_cfl, then, when clock is not NULL,
+ * the output-time clamp. Waits for the stream; writes the result to *dt_out. */
+mc_status mc_compute_dt(mc_ctx* ctx, const double* Q, const mc_clock* clock, double* dt_out,
+                        void* stream);
+
+/* time_step (source/TimeStepping.cpp:39-308): one SSPRK step of size dt in
+ * place on Q (ghosts filled on entry and on exit). Each stage is one fused
+ * kernel (two in 3D). The CFL minimum of the new state is reduced in the
+ * last stage and can be read with mc_last_cfl_min. */
+mc_status mc_time_step(mc_ctx* ctx, double* Q, double dt, void* stream);
+
+/* The main loop of source/main.cpp:54-72 on the device: up to max_steps of
+ * { dt = compute_dt; time_step(dt); time += dt } stopping after the step
+ * that reaches max_time or an output time (prev_output_time + output_delta),
+ * where prev_output_time becomes time. The first dt is computed from Q; later
+ * ones are fused into each step's last stage. dt and time never leave the
+ * GPU inside the loop; on return (after waiting for the stream) *clock holds
+ * the new clock, *steps_done the steps taken and, if dt_log is not NULL,
+ * dt_log[0..steps_done) the dt of each step. */
+mc_status mc_advance(mc_ctx* ctx, double* Q, mc_clock* clock, int64_t max_steps,
+                     int64_t* steps_done, double* dt_log, void* stream);
+
+/* Raw CFL minimum (before max_cfl) of the state written by the last
+ * mc_time_step / mc_advance step. Waits for the stream. */
+mc_status mc_last_cfl_min(mc_ctx* ctx, double* cfl_min, void* stream);
+
+/* Physics flags (MC_FLAG_*) accumulated since the last call; clears them.
+ * Waits for the stream. */
+mc_status mc_get_status(mc_ctx* ctx, uint32_t* flags, void* stream);
+
+/* Kernel timing with CUDA events recorded on the launch stream around every
+ * stage kernel (kind 0: the fused stage kernel, or in 3D its x-y plane pass;
+ * kind 1: the 3D z pass). mc_profile_stages(ctx, 1) starts recording (and
+ * clears earlier records), 0 stops. mc_stage_time waits for the recorded
+ * events and returns the summed kernel time in milliseconds and the number of
+ * launches of that kind. */
+mc_status mc_profile_stages(mc_ctx* ctx, int32_t enable);
+mc_status mc_stage_time(mc_ctx* ctx, int32_t kind, double* total_ms, int64_t* launches);
+
+/* Number of kernel launches issued by this context since it was created. */
+int64_t mc_launch_count(const mc_ctx* ctx);
+
+/* Message of the last failed call on this thread (static storage). */
+const char* mc_last_error(void);
+
+int32_t mc_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOSSCAP_B200_H */

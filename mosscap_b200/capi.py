@@ -1,0 +1,129 @@
+"""ctypes binding of the C ABI in ``include/mosscap_b200.h``.
+
+The shared library is ``mosscap_b200/libmosscap_b200.so`` (built by
+``mosscap_b200.build``). Loading fails loudly when it is missing: there is no
+fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+from typing import List
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libmosscap_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "mosscap_b200.h")
+
+MC_OK = 0
+STATUS_NAMES = {0: "MC_OK", 1: "MC_ERR_INVALID_ARGUMENT", 2: "MC_ERR_UNSUPPORTED", 3: "MC_ERR_CUDA",
+                4: "MC_ERR_OUT_OF_MEMORY", 5: "MC_ERR_STATE"}
+FLAG_NONFINITE, FLAG_NEG_DENSITY, FLAG_NEG_PRESSURE, FLAG_BAD_DT = 0x1, 0x2, 0x4, 0x8
+
+RECON = {"fog": 0, "muscl": 1, "ppm": 2, "weno5z": 3}
+LIMITER = {"vanleer": 0, "monotonizedcentral": 1, "minmod": 2}
+RIEMANN = {"rusanov": 0, "hll": 1, "hllc": 2}
+STEPPER = {"rk2": 0, "ssprk3": 1, "ssprk4": 2}
+BOUNDARY = {"wall": 0, "periodic": 1, "symmetric": 2, "symmetricoutflowdiode": 3,
+            "zerograd": 4, "constant": 5, "userfn": 6}
+PRECISION = {"fp64": 0, "fp32": 1}
+
+
+class McGrid(ctypes.Structure):
+    _fields_ = [
+        ("num_dim", ctypes.c_int32),
+        ("xc", ctypes.c_int32), ("yc", ctypes.c_int32), ("zc", ctypes.c_int32),
+        ("ng", ctypes.c_int32),
+        ("num_tracers", ctypes.c_int32),
+        ("dx", ctypes.c_double),
+        ("loc", ctypes.c_double * 3),
+        ("bc", ctypes.c_int32 * 6),
+        ("bc_const", (ctypes.c_double * 5) * 6),
+    ]
+
+
+class McScheme(ctypes.Structure):
+    _fields_ = [
+        ("reconstruction", ctypes.c_int32),
+        ("slope_limiter", ctypes.c_int32),
+        ("riemann_solver", ctypes.c_int32),
+        ("time_stepper", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("gamma", ctypes.c_double),
+        ("max_cfl", ctypes.c_double),
+    ]
+
+
+class McClock(ctypes.Structure):
+    _fields_ = [
+        ("time", ctypes.c_double),
+        ("max_time", ctypes.c_double),
+        ("prev_output_time", ctypes.c_double),
+        ("output_delta", ctypes.c_double),
+    ]
+
+
+USER_BC_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
+
+
+class McError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_LIB = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the C-ABI library (raises if it was not built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is missing; build it with python -m mosscap_b200.build")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64, d = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    P = ctypes.POINTER
+    lib.mc_abi_version.restype = i32
+    lib.mc_last_error.restype = ctypes.c_char_p
+    lib.mc_create.argtypes = [P(McGrid), P(McScheme), P(vp)]
+    lib.mc_create.restype = i32
+    lib.mc_destroy.argtypes = [vp]
+    lib.mc_destroy.restype = i32
+    lib.mc_set_user_bc.argtypes = [vp, USER_BC_FN, vp]
+    lib.mc_set_user_bc.restype = i32
+    lib.mc_fill_bcs.argtypes = [vp, vp, vp]
+    lib.mc_fill_bcs.restype = i32
+    lib.mc_compute_dt.argtypes = [vp, vp, P(McClock), P(d), vp]
+    lib.mc_compute_dt.restype = i32
+    lib.mc_time_step.argtypes = [vp, vp, d, vp]
+    lib.mc_time_step.restype = i32
+    lib.mc_advance.argtypes = [vp, vp, P(McClock), i64, P(i64), P(d), vp]
+    lib.mc_advance.restype = i32
+    lib.mc_last_cfl_min.argtypes = [vp, P(d), vp]
+    lib.mc_last_cfl_min.restype = i32
+    lib.mc_get_status.argtypes = [vp, P(ctypes.c_uint32), vp]
+    lib.mc_get_status.restype = i32
+    lib.mc_profile_stages.argtypes = [vp, i32]
+    lib.mc_profile_stages.restype = i32
+    lib.mc_stage_time.argtypes = [vp, i32, P(d), P(i64)]
+    lib.mc_stage_time.restype = i32
+    lib.mc_launch_count.argtypes = [vp]
+    lib.mc_launch_count.restype = i64
+    if lib.mc_abi_version() != 1:
+        raise RuntimeError("unexpected ABI version")
+    _LIB = lib
+    return lib
+
+
+def check(status: int, where: str) -> None:
+    if status != MC_OK:
+        raise McError(status, where, load().mc_last_error().decode())
+
+
+def declared_functions(header: str = HEADER) -> List[str]:
+    """Names of the functions ``include/mosscap_b200.h`` declares."""
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(mc_[a-z_0-9]+)\s*\(", text)))

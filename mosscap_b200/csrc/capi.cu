@@ -1,0 +1,550 @@
+// C ABI of the library (include/mosscap_b200.h): context management, stage
+// sequencing of the SSPRK drivers and the device-driven main loop.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "launch.h"
+#include "mosscap_b200.h"
+
+using mc::StageParams;
+
+struct mc_ctx {
+    mc_grid grid;
+    mc_scheme scheme;
+    int device = 0;
+    int nx = 1, ny = 1, nz = 1, nvar = 0;
+    long long plane = 0;          // cells per variable, ghosts included
+    size_t state_bytes = 0;
+    double* buf_a = nullptr;      // stage buffers
+    double* buf_b = nullptr;
+    double* dqxy = nullptr;       // 3D x+y divergence
+    mc::DeviceBlock* blk = nullptr;
+    mc::DeviceBlock* blk_host = nullptr;  // pinned mirror for read-back
+    double* dt_log = nullptr;     // device dt log of mc_advance
+    int64_t dt_log_cap = 0;
+    int64_t launches = 0;
+    bool min_from_clock = false;  // last CFL minimum sits in blk->last_cfl_min
+    void (*user_bc)(void*, double*, void*) = nullptr;
+    void* user_bc_data = nullptr;
+    // kernel timing (mc_profile_stages)
+    bool profiling = false;
+    struct Timed {
+        cudaEvent_t start, stop;
+        int kind;
+    };
+    std::vector<Timed> timed;
+    std::vector<cudaEvent_t> event_pool;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+mc_status fail(mc_status s, const std::string& msg) {
+    g_error = msg;
+    return s;
+}
+
+mc_status cuda_fail(cudaError_t e, const char* where) {
+    return fail(MC_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define MC_CUDA(call, where)                   \
+    do {                                       \
+        cudaError_t e_ = (call);               \
+        if (e_ != cudaSuccess) {               \
+            return cuda_fail(e_, where);       \
+        }                                      \
+    } while (0)
+
+int halo_needed(int rec) {
+    return rec == MC_RECON_FOG ? 1 : rec == MC_RECON_MUSCL ? 2 : 3;
+}
+
+// The stage plan of each SSPRK driver (source/TimeStepping.cpp): input and
+// output buffer of each stage (0 = caller's Q, 1 = buffer A, 2 = buffer B)
+// and the combination applied.
+struct StagePlan {
+    int n;
+    int in[4], out[4], combo[4];
+};
+
+StagePlan plan_for(int stepper) {
+    switch (stepper) {
+        case MC_STEPPER_RK2:
+            return {2, {0, 1}, {1, 0}, {mc::kAdd, mc::kRk2Final}};
+        case MC_STEPPER_SSPRK3:
+            return {3, {0, 1, 2}, {1, 2, 0}, {mc::kAdd, mc::kSsp3Second, mc::kSsp3Final}};
+        default:
+            return {4, {0, 1, 2, 1}, {1, 2, 1, 0}, {mc::kHalfAdd, mc::kHalfAdd, mc::kSsp4Third, mc::kHalfAdd}};
+    }
+}
+
+StageParams base_params(const mc_ctx* c) {
+    StageParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.xc = c->grid.xc;
+    p.yc = c->grid.yc;
+    p.zc = c->grid.zc;
+    p.ng = c->grid.ng;
+    p.nx = c->nx;
+    p.ny = c->ny;
+    p.nz = c->nz;
+    p.nvar = c->nvar;
+    p.ntracer = c->grid.num_tracers;
+    p.plane = c->plane;
+    p.dx = c->grid.dx;
+    p.gamma = c->scheme.gamma;
+    p.blk = c->blk;
+    for (int f = 0; f < 6; ++f) {
+        p.bc.kind[f] = c->grid.bc[f];
+        for (int v = 0; v < mc::kMaxVars; ++v) {
+            p.bc.cval[f][v] = v < 5 ? c->grid.bc_const[f][v] : 0.0;
+        }
+    }
+    return p;
+}
+
+cudaEvent_t pooled_event(mc_ctx* c) {
+    if (!c->event_pool.empty()) {
+        cudaEvent_t e = c->event_pool.back();
+        c->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+cudaError_t launch_stage_kernel(mc_ctx* c, const StageParams& p, int pass, cudaStream_t s);
+
+// Launch one stage kernel; with profiling on, bracket it with events.
+cudaError_t launch_stage(mc_ctx* c, const StageParams& p, int pass, cudaStream_t s) {
+    if (!c->profiling) {
+        return launch_stage_kernel(c, p, pass, s);
+    }
+    mc_ctx::Timed t{pooled_event(c), pooled_event(c), c->grid.num_dim == 3 ? pass : 0};
+    cudaEventRecord(t.start, s);
+    const cudaError_t e = launch_stage_kernel(c, p, pass, s);
+    cudaEventRecord(t.stop, s);
+    c->timed.push_back(t);
+    return e;
+}
+
+cudaError_t launch_stage_kernel(mc_ctx* c, const StageParams& p, int pass, cudaStream_t s) {
+    const int nd = c->grid.num_dim;
+    const bool f32 = c->scheme.precision == MC_PRECISION_FP32_COMPENSATED;
+    const int r = c->scheme.reconstruction, l = c->scheme.slope_limiter, rs = c->scheme.riemann_solver;
+    c->launches += 1;
+    if (nd == 1) {
+        return f32 ? mc::launch_stage_d1_fp32(p, r, l, rs, pass, s) : mc::launch_stage_d1_fp64(p, r, l, rs, pass, s);
+    }
+    if (nd == 2) {
+        return f32 ? mc::launch_stage_d2_fp32(p, r, l, rs, pass, s) : mc::launch_stage_d2_fp64(p, r, l, rs, pass, s);
+    }
+    return f32 ? mc::launch_stage_d3_fp32(p, r, l, rs, pass, s) : mc::launch_stage_d3_fp64(p, r, l, rs, pass, s);
+}
+
+// Enqueue one SSPRK step on Q. dt_dev (device-driven loop) or dt (host).
+mc_status enqueue_step(mc_ctx* c, double* Q, double dt, const double* dt_dev, bool reset_min, cudaStream_t s) {
+    const StagePlan plan = plan_for(c->scheme.time_stepper);
+    double* bufs[3] = {Q, c->buf_a, c->buf_b};
+    for (int st = 0; st < plan.n; ++st) {
+        StageParams p = base_params(c);
+        p.q_in = bufs[plan.in[st]];
+        p.q_old = Q;
+        p.q_out = bufs[plan.out[st]];
+        p.dqxy = c->dqxy;
+        p.dt = dt;
+        p.dt_dev = dt_dev;
+        p.combo = plan.combo[st];
+        p.last = st == plan.n - 1;
+        p.reset_min = (reset_min && st == 0) ? 1 : 0;
+        MC_CUDA(launch_stage(c, p, 0, s), "stage launch");
+        if (c->grid.num_dim == 3) {
+            p.reset_min = 0;
+            MC_CUDA(launch_stage(c, p, 1, s), "stage launch (z pass)");
+        }
+        if (c->user_bc) {
+            c->user_bc(c->user_bc_data, p.q_out, (void*)s);
+        }
+    }
+    return MC_OK;
+}
+
+double clamp_to_output(double dt, const mc_clock* k) {
+    // source/Hydro.cpp:231-241
+    const double cand = k->prev_output_time + k->output_delta;
+    const double next_write = (cand < k->max_time) ? cand : k->max_time;
+    if (k->time + dt >= next_write) {
+        dt = next_write - k->time;
+        while (k->time + dt < next_write) {
+            dt = std::nextafter(dt, DBL_MAX);
+        }
+    }
+    return dt;
+}
+
+mc_status check_ctx(const mc_ctx* c) {
+    if (!c) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null context");
+    }
+    return MC_OK;
+}
+
+// A MC_BC_USERFN face is filled only by the caller's hook.
+mc_status check_user_bc(const mc_ctx* c) {
+    for (int f = 0; f < 2 * c->grid.num_dim; ++f) {
+        if (c->grid.bc[f] == MC_BC_USERFN && !c->user_bc) {
+            return fail(MC_ERR_INVALID_ARGUMENT, "a MC_BC_USERFN face needs mc_set_user_bc");
+        }
+    }
+    return MC_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int32_t mc_abi_version(void) {
+    return MC_ABI_VERSION;
+}
+
+const char* mc_last_error(void) {
+    return g_error.c_str();
+}
+
+mc_status mc_create(const mc_grid* grid, const mc_scheme* scheme, mc_ctx** out) {
+    if (!grid || !scheme || !out) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    *out = nullptr;
+    const mc_grid& g = *grid;
+    const mc_scheme& s = *scheme;
+    if (g.num_dim < 1 || g.num_dim > 3) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "num_dim must be 1, 2 or 3");
+    }
+    if (s.reconstruction < 0 || s.reconstruction > 3 || s.slope_limiter < 0 || s.slope_limiter > 2 ||
+        s.riemann_solver < 0 || s.riemann_solver > 2 || s.time_stepper < 0 || s.time_stepper > 2 ||
+        s.precision < 0 || s.precision > 1) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "scheme enum out of range");
+    }
+    if (g.ng < halo_needed(s.reconstruction) || g.ng > mc::kMaxGhost) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "ng below the reconstruction's need or above 8");
+    }
+    const int ext[3] = {g.xc, g.yc, g.zc};
+    for (int a = 0; a < 3; ++a) {
+        if (a < g.num_dim) {
+            if (ext[a] - 2 * g.ng < g.ng) {
+                return fail(MC_ERR_INVALID_ARGUMENT, "each active axis needs at least ng interior cells");
+            }
+        } else if (ext[a] != 1) {
+            return fail(MC_ERR_INVALID_ARGUMENT, "inactive axes must have extent 1");
+        }
+    }
+    if (g.num_tracers < 0 || 2 + g.num_dim + g.num_tracers > mc::kMaxVars) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "too many variables (at most 8)");
+    }
+    if (g.num_dim == 3 && g.num_tracers > 0) {
+        return fail(MC_ERR_UNSUPPORTED, "passive tracers are not implemented in 3D");
+    }
+    if (!(g.dx > 0.0) || !std::isfinite(g.dx) || !std::isfinite(s.gamma) || !std::isfinite(s.max_cfl)) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "dx, gamma and max_cfl must be finite (dx > 0)");
+    }
+    for (int f = 0; f < 2 * g.num_dim; ++f) {
+        if (g.bc[f] < 0 || g.bc[f] > MC_BC_USERFN) {
+            return fail(MC_ERR_INVALID_ARGUMENT, "boundary kind out of range");
+        }
+        if (g.bc[f] == MC_BC_CONSTANT && 2 + g.num_dim + g.num_tracers > 5) {
+            return fail(MC_ERR_UNSUPPORTED, "constant boundaries hold at most 5 variables");
+        }
+    }
+    if ((g.bc[0] == MC_BC_PERIODIC) != (g.bc[1] == MC_BC_PERIODIC) ||
+        (g.num_dim > 1 && (g.bc[2] == MC_BC_PERIODIC) != (g.bc[3] == MC_BC_PERIODIC)) ||
+        (g.num_dim > 2 && (g.bc[4] == MC_BC_PERIODIC) != (g.bc[5] == MC_BC_PERIODIC))) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "periodic boundaries come in pairs");
+    }
+    mc_ctx* c = new (std::nothrow) mc_ctx();
+    if (!c) {
+        return fail(MC_ERR_OUT_OF_MEMORY, "host allocation");
+    }
+    c->grid = g;
+    // unused axes: keep their kinds out of the ghost logic
+    for (int f = 2 * g.num_dim; f < 6; ++f) {
+        c->grid.bc[f] = MC_BC_USERFN;
+    }
+    c->scheme = s;
+    cudaGetDevice(&c->device);
+    c->nx = g.xc - 2 * g.ng;
+    c->ny = g.num_dim > 1 ? g.yc - 2 * g.ng : 1;
+    c->nz = g.num_dim > 2 ? g.zc - 2 * g.ng : 1;
+    c->nvar = 2 + g.num_dim + g.num_tracers;
+    c->plane = (long long)g.xc * g.yc * g.zc;
+    c->state_bytes = sizeof(double) * (size_t)c->nvar * (size_t)c->plane;
+    cudaError_t e = cudaMalloc(&c->buf_a, c->state_bytes);
+    if (e == cudaSuccess) {
+        e = cudaMalloc(&c->buf_b, c->state_bytes);
+    }
+    if (e == cudaSuccess && g.num_dim == 3) {
+        e = cudaMalloc(&c->dqxy, sizeof(double) * (size_t)c->nvar * c->nx * c->ny * c->nz);
+    }
+    if (e == cudaSuccess) {
+        e = cudaMalloc(&c->blk, sizeof(mc::DeviceBlock));
+    }
+    if (e == cudaSuccess) {
+        e = cudaMallocHost(&c->blk_host, sizeof(mc::DeviceBlock));
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemset(c->blk, 0, sizeof(mc::DeviceBlock));
+    }
+    if (e != cudaSuccess) {
+        mc_destroy(c);
+        return e == cudaErrorMemoryAllocation ? fail(MC_ERR_OUT_OF_MEMORY, "device allocation")
+                                              : cuda_fail(e, "mc_create");
+    }
+    *out = c;
+    return MC_OK;
+}
+
+mc_status mc_destroy(mc_ctx* c) {
+    if (!c) {
+        return MC_OK;
+    }
+    cudaFree(c->buf_a);
+    cudaFree(c->buf_b);
+    cudaFree(c->dqxy);
+    cudaFree(c->blk);
+    cudaFree(c->dt_log);
+    if (c->blk_host) {
+        cudaFreeHost(c->blk_host);
+    }
+    for (auto& t : c->timed) {
+        cudaEventDestroy(t.start);
+        cudaEventDestroy(t.stop);
+    }
+    for (auto e : c->event_pool) {
+        cudaEventDestroy(e);
+    }
+    delete c;
+    return MC_OK;
+}
+
+mc_status mc_set_user_bc(mc_ctx* c, void (*fn)(void* user, double* Q, void* stream), void* user) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    c->user_bc = fn;
+    c->user_bc_data = user;
+    return MC_OK;
+}
+
+mc_status mc_fill_bcs(mc_ctx* c, double* Q, void* stream) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    if (!Q) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null Q");
+    }
+    StageParams p = base_params(c);
+    p.q_in = Q;
+    p.q_out = Q;
+    c->launches += 1;
+    MC_CUDA(mc::launch_fill_bcs(p, c->grid.num_dim, (cudaStream_t)stream), "fill_bcs");
+    if (c->user_bc) {
+        c->user_bc(c->user_bc_data, Q, stream);
+    }
+    return MC_OK;
+}
+
+mc_status mc_compute_dt(mc_ctx* c, const double* Q, const mc_clock* clock, double* dt_out, void* stream) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    if (!Q || !dt_out) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    const cudaStream_t s = (cudaStream_t)stream;
+    StageParams p = base_params(c);
+    p.q_in = Q;
+    c->launches += 2;
+    MC_CUDA(mc::launch_cfl_min(p, c->grid.num_dim, s), "cfl_min");
+    MC_CUDA(cudaMemcpyAsync(c->blk_host, c->blk, sizeof(mc::DeviceBlock), cudaMemcpyDeviceToHost, s), "read-back");
+    MC_CUDA(cudaStreamSynchronize(s), "sync");
+    double m;
+    std::memcpy(&m, &c->blk_host->cfl_min_bits, sizeof(double));
+    double dt = m * c->scheme.max_cfl;
+    if (clock) {
+        dt = clamp_to_output(dt, clock);
+    }
+    *dt_out = dt;
+    return MC_OK;
+}
+
+mc_status mc_time_step(mc_ctx* c, double* Q, double dt, void* stream) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    if (!Q) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null Q");
+    }
+    if (!(dt > 0.0) || !std::isfinite(dt)) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "dt must be positive and finite");
+    }
+    if (mc_status st = check_user_bc(c)) {
+        return st;
+    }
+    c->min_from_clock = false;
+    return enqueue_step(c, Q, dt, nullptr, true, (cudaStream_t)stream);
+}
+
+mc_status mc_advance(mc_ctx* c, double* Q, mc_clock* clock, int64_t max_steps, int64_t* steps_done,
+                     double* dt_log, void* stream) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    if (!Q || !clock || max_steps < 0) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null Q / clock or negative max_steps");
+    }
+    if (mc_status st = check_user_bc(c)) {
+        return st;
+    }
+    const cudaStream_t s = (cudaStream_t)stream;
+    if (dt_log && c->dt_log_cap < max_steps + 1) {
+        cudaFree(c->dt_log);
+        c->dt_log = nullptr;
+        c->dt_log_cap = 0;
+        MC_CUDA(cudaMalloc(&c->dt_log, sizeof(double) * (size_t)(max_steps + 1)), "dt log");
+        c->dt_log_cap = max_steps + 1;
+    }
+    double* dlog = dt_log ? c->dt_log : nullptr;
+    c->min_from_clock = true;
+    MC_CUDA(mc::launch_clock_init(c->blk, clock->time, clock->max_time, clock->prev_output_time,
+                                  clock->output_delta, c->scheme.max_cfl, s),
+            "clock init");
+    StageParams p = base_params(c);
+    p.q_in = Q;
+    MC_CUDA(mc::launch_cfl_min(p, c->grid.num_dim, s), "cfl_min");
+    MC_CUDA(mc::launch_clock_advance(c->blk, dlog, 1, s), "clock");
+    c->launches += 4;
+    const double* dt_dev = &c->blk->dt;
+    const int64_t chunk = 64;
+    int64_t issued = 0;
+    while (issued < max_steps) {
+        const int64_t n = std::min(chunk, max_steps - issued);
+        for (int64_t k = 0; k < n; ++k) {
+            if (mc_status st = enqueue_step(c, Q, 0.0, dt_dev, false, s)) {
+                return st;
+            }
+            MC_CUDA(mc::launch_clock_advance(c->blk, dlog, 0, s), "clock");
+            c->launches += 1;
+        }
+        issued += n;
+        if (issued < max_steps) {
+            MC_CUDA(cudaMemcpyAsync(c->blk_host, c->blk, sizeof(mc::DeviceBlock), cudaMemcpyDeviceToHost, s),
+                    "read-back");
+            MC_CUDA(cudaStreamSynchronize(s), "sync");
+            if (c->blk_host->done) {
+                break;
+            }
+        }
+    }
+    MC_CUDA(cudaMemcpyAsync(c->blk_host, c->blk, sizeof(mc::DeviceBlock), cudaMemcpyDeviceToHost, s), "read-back");
+    MC_CUDA(cudaStreamSynchronize(s), "sync");
+    const mc::DeviceBlock& b = *c->blk_host;
+    clock->time = b.time;
+    clock->prev_output_time = b.prev_output_time;
+    if (steps_done) {
+        *steps_done = b.steps;
+    }
+    if (dt_log && b.steps > 0) {
+        MC_CUDA(cudaMemcpy(dt_log, c->dt_log, sizeof(double) * (size_t)b.steps, cudaMemcpyDeviceToHost),
+                "dt log read-back");
+    }
+    return MC_OK;
+}
+
+mc_status mc_last_cfl_min(mc_ctx* c, double* cfl_min, void* stream) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    if (!cfl_min) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    const cudaStream_t s = (cudaStream_t)stream;
+    MC_CUDA(cudaMemcpyAsync(c->blk_host, c->blk, sizeof(mc::DeviceBlock), cudaMemcpyDeviceToHost, s), "read-back");
+    MC_CUDA(cudaStreamSynchronize(s), "sync");
+    if (c->min_from_clock) {
+        *cfl_min = c->blk_host->last_cfl_min;
+    } else {
+        std::memcpy(cfl_min, &c->blk_host->cfl_min_bits, sizeof(double));
+    }
+    return MC_OK;
+}
+
+mc_status mc_get_status(mc_ctx* c, uint32_t* flags, void* stream) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    if (!flags) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    const cudaStream_t s = (cudaStream_t)stream;
+    MC_CUDA(cudaMemcpyAsync(c->blk_host, c->blk, sizeof(mc::DeviceBlock), cudaMemcpyDeviceToHost, s), "read-back");
+    MC_CUDA(cudaStreamSynchronize(s), "sync");
+    *flags = c->blk_host->status;
+    const unsigned zero = 0;
+    MC_CUDA(cudaMemcpyAsync(&c->blk->status, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, s), "clear");
+    MC_CUDA(cudaStreamSynchronize(s), "sync");
+    return MC_OK;
+}
+
+mc_status mc_profile_stages(mc_ctx* c, int32_t enable) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    for (auto& t : c->timed) {
+        c->event_pool.push_back(t.start);
+        c->event_pool.push_back(t.stop);
+    }
+    c->timed.clear();
+    c->profiling = enable != 0;
+    return MC_OK;
+}
+
+mc_status mc_stage_time(mc_ctx* c, int32_t kind, double* total_ms, int64_t* launches) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    if (!total_ms || !launches) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    double sum = 0.0;
+    int64_t n = 0;
+    for (auto& t : c->timed) {
+        if (t.kind != kind) {
+            continue;
+        }
+        MC_CUDA(cudaEventSynchronize(t.stop), "event sync");
+        float ms = 0.0f;
+        MC_CUDA(cudaEventElapsedTime(&ms, t.start, t.stop), "event time");
+        sum += ms;
+        ++n;
+    }
+    *total_ms = sum;
+    *launches = n;
+    return MC_OK;
+}
+
+int64_t mc_launch_count(const mc_ctx* c) {
+    return c ? c->launches : 0;
+}
+
+} // extern "C"

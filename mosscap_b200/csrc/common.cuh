@@ -1,0 +1,264 @@
+// Shared device-side definitions of the Euler-step kernels: launch
+// parameters, the device control block, SSPRK stage combinations, boundary
+// transforms and the order-preserving CFL minimum.
+#pragma once
+
+#include <cstdint>
+
+#include "physics.cuh"
+
+namespace mc {
+
+constexpr int kMaxVars = 8;   // 2 + num_dim hydro variables plus tracers
+constexpr int kMaxGhost = 8;  // ghost cells per side accepted by the library
+
+enum Bc : int { kWall = 0, kPeriodic, kSymmetric, kDiode, kZeroGrad, kConstant, kUserFn };
+
+// Stage combinations of the SSPRK drivers (source/TimeStepping.cpp).
+enum Combo : int {
+    kAdd = 0,        // Q_in + (L + S)              rk2 0, ssprk3 0        :66, :143
+    kRk2Final,       // 0.5 (Q_old + Q_in + L + S)  rk2 1                  :86
+    kSsp3Second,     // 3/4 Q_old + 1/4 (Q_in + L + S)      ssprk3 1       :163
+    kSsp3Final,      // 1/3 Q_old + 2/3 (Q_in + L + S)      ssprk3 2       :183
+    kHalfAdd,        // Q_in + 1/2 (L + S)          ssprk4 0, 1, 3         :240, :260, :300
+    kSsp4Third       // 2/3 Q_old + 1/3 Q_in + 1/6 (L + S)  ssprk4 2       :280
+};
+
+// Device control block: one per context, in device memory.
+struct DeviceBlock {
+    unsigned long long cfl_min_bits;  // atomicMin target: bits of a non-negative double
+    double dt;                        // dt of the step in flight (device-driven loop)
+    double time;
+    double prev_output_time;
+    double max_time;
+    double output_delta;
+    double max_cfl;
+    double last_cfl_min;              // CFL minimum of the last completed step
+    long long steps;                  // steps taken by the device-driven loop
+    int done;                         // nonzero: the device-driven loop has stopped
+    unsigned status;                  // MC_FLAG_* bits
+};
+
+struct BcDesc {
+    int kind[6];            // xs, xe, ys, ye, zs, ze
+    double cval[6][kMaxVars];
+};
+
+// Launch parameters of one stage.
+struct StageParams {
+    const double* __restrict__ q_in;  // stage input, ghosts filled
+    const double* q_old;              // step-start state, read only at the written cell
+    double* q_out;                    // stage output (interior and ghosts)
+    double* dqxy;                     // 3D only: x+y flux divergence per interior cell
+    int xc, yc, zc, ng;
+    int nx, ny, nz;                   // interior extents
+    int nvar, ntracer;
+    long long plane;                  // xc * yc * zc
+    double dx, gamma;
+    double dt;                        // used when dt_dev is null
+    const double* dt_dev;             // device dt (the device-driven loop)
+    int combo;
+    int last;                         // nonzero in the last stage: CFL minimum + checks
+    int reset_min;                    // nonzero: reset blk->cfl_min_bits (a stage before the last)
+    BcDesc bc;
+    DeviceBlock* blk;
+};
+
+constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;
+
+// Called at the top of every stage kernel: a stage that is not the last one
+// clears the CFL-minimum cell that the last stage will reduce into.
+__device__ __forceinline__ void maybe_reset_min(const StageParams& p) {
+    if (p.reset_min && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 &&
+        threadIdx.y == 0 && threadIdx.z == 0) {
+        p.blk->cfl_min_bits = kInfBits;
+    }
+}
+
+__device__ __forceinline__ double stage_dt(const StageParams& p) {
+    return p.dt_dev ? *p.dt_dev : p.dt;
+}
+
+// One SSPRK stage update of one variable; qu is the flux divergence already
+// multiplied by dt/dx and src the source term times dt.
+__device__ __forceinline__ double combine(int combo, double q_old, double q_in, double qu, double src) {
+    switch (combo) {
+        case kAdd:
+            return q_in + (qu + src);
+        case kRk2Final:
+            return 0.5 * (q_old + q_in + qu + src);
+        case kSsp3Second:
+            return 0.75 * q_old + 0.25 * (q_in + qu + src);
+        case kSsp3Final:
+            return (1.0 / 3.0) * q_old + (2.0 / 3.0) * (q_in + qu + src);
+        case kHalfAdd:
+            return q_in + 0.5 * (qu + src);
+        default:
+            return (2.0 / 3.0) * q_old + (1.0 / 3.0) * q_in + (1.0 / 6.0) * (qu + src);
+    }
+}
+
+__host__ __device__ inline bool combo_reads_old(int combo) {
+    return combo == kRk2Final || combo == kSsp3Second || combo == kSsp3Final || combo == kSsp4Third;
+}
+
+// ---- Boundary conditions as a scatter ----------------------------------------
+//
+// fill_bcs (source/Boundaries.hpp:11-149) fills x ghosts, then y ghosts over
+// the full x extent, then z ghosts over the full x-y extent. Every ghost value
+// it produces is a transform of one interior cell: ghost (gx, gy, gz) ends up
+// as Tz(Ty(Tx(Q[sz][sy][sx]))), where along each axis s is the source index
+// of the ghost (itself for interior indices) and T the face's transform
+// (identity for interior indices). The kernels below therefore write, next to
+// each interior cell they update, every ghost whose source it is.
+
+// Ghost targets of array index c along one axis. Entry 0 is c itself
+// (no transform). face[] is -1 for c itself, 0 for the start face, 1 for the
+// end face. n interior cells, ng ghosts, requires n >= ng.
+__device__ __forceinline__ int axis_targets(int c, int n, int ng, int bs, int be, int* idx, int* face) {
+    int cnt = 0;
+    idx[cnt] = c;
+    face[cnt++] = -1;
+    // start face: ghosts 0..ng-1
+    if (bs == kPeriodic) {
+        if (c >= n && c < n + ng) {  // ghost g takes g + n
+            idx[cnt] = c - n;
+            face[cnt++] = 0;
+        }
+    } else if (bs == kWall || bs == kSymmetric || bs == kDiode) {
+        if (c >= ng && c < 2 * ng) {  // mirror about the face
+            idx[cnt] = 2 * ng - 1 - c;
+            face[cnt++] = 0;
+        }
+    } else if (bs == kZeroGrad || bs == kConstant) {
+        if (c == ng) {
+            for (int g = 0; g < ng; ++g) {
+                idx[cnt] = g;
+                face[cnt++] = 0;
+            }
+        }
+    }
+    // end face: ghosts ng+n .. 2ng+n-1
+    if (be == kPeriodic) {
+        if (c >= ng && c < 2 * ng) {
+            idx[cnt] = c + n;
+            face[cnt++] = 1;
+        }
+    } else if (be == kWall || be == kSymmetric || be == kDiode) {
+        if (c >= n && c < n + ng) {
+            idx[cnt] = 2 * (ng + n) - 1 - c;
+            face[cnt++] = 1;
+        }
+    } else if (be == kZeroGrad || be == kConstant) {
+        if (c == ng + n - 1) {
+            for (int g = 0; g < ng; ++g) {
+                idx[cnt] = ng + n + g;
+                face[cnt++] = 1;
+            }
+        }
+    }
+    return cnt;
+}
+
+// Whether array index c along an axis feeds any ghost (fast-path test).
+__device__ __forceinline__ bool near_face(int c, int n, int ng) {
+    return c < 2 * ng || c >= n;
+}
+
+// Apply the transform of face `face` (0 start, 1 end) of axis `axis`
+// to a conserved vector                                   Boundaries.hpp:83-115
+template <int NDIM>
+__device__ __forceinline__ void bc_transform(const BcDesc& bc, int axis, int face, int nvar, double* q) {
+    const int kind = bc.kind[2 * axis + face];
+    const int im = 1 + axis;
+    constexpr int ie = 1 + NDIM;
+    if (kind == kWall) {
+        q[im] = -q[im];
+    } else if (kind == kDiode) {
+        const double mom_pre = q[im];
+        q[im] = face == 0 ? smin(mom_pre, 0.0) : smax(mom_pre, 0.0);
+        q[ie] -= sq(q[im] - mom_pre) / q[0];
+    } else if (kind == kConstant) {
+#pragma unroll
+        for (int v = 0; v < kMaxVars; ++v) {
+            if (v < nvar) {
+                q[v] = bc.cval[2 * axis + face][v];
+            }
+        }
+    }
+}
+
+// ---- Status checks and the CFL minimum ----------------------------------------
+
+__device__ __forceinline__ unsigned state_flags(double rho, double p, bool finite) {
+    unsigned f = 0;
+    if (!finite) {
+        f |= 0x1u;
+    }
+    if (!(rho > 0.0)) {
+        f |= 0x2u;
+    }
+    if (!(p > 0.0)) {
+        f |= 0x4u;
+    }
+    return f;
+}
+
+// Non-negative doubles (and +inf) order like their bit patterns read as
+// unsigned integers, so an integer atomicMin on the bits is an exact,
+// order-independent floating-point minimum. NaN is mapped to +inf bits (and
+// flagged separately).
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+    if (!(v == v)) {
+        return 0x7ff0000000000000ull;
+    }
+    if (v <= 0.0) {
+        return 0ull;
+    }
+    return static_cast<unsigned long long>(__double_as_longlong(v));
+}
+
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v = smin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+__device__ __forceinline__ unsigned warp_or(unsigned v) {
+    return __reduce_or_sync(0xffffffffu, v);
+}
+
+// Block-wide min of v and OR of flags; thread 0 publishes both with one
+// atomic each. red_d / red_u hold one entry per warp of the block.
+__device__ __forceinline__ void block_publish(double v, unsigned flags, bool do_min, DeviceBlock* blk,
+                                              double* red_d, unsigned* red_u) {
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nw = (blockDim.x * blockDim.y * blockDim.z) >> 5;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    v = warp_min(v);
+    flags = warp_or(flags);
+    if (lane == 0) {
+        red_d[warp] = v;
+        red_u[warp] = flags;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double m = red_d[0];
+        unsigned f = red_u[0];
+        for (int w = 1; w < nw; ++w) {
+            m = smin(m, red_d[w]);
+            f |= red_u[w];
+        }
+        if (do_min) {
+            atomicMin(&blk->cfl_min_bits, ordered_bits(m));
+        }
+        if (f) {
+            atomicOr(&blk->status, f);
+        }
+    }
+}
+
+} // namespace mc

@@ -1,0 +1,29 @@
+// Host-side declarations of the kernel launchers (csrc/*.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace mc {
+
+// One stage of an SSPRK step. pass selects, in 3D, the x-y plane pass (0)
+// or the z pass that finishes the stage (1); it is ignored in 1D and 2D.
+cudaError_t launch_stage_d1_fp64(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d2_fp64(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d3_fp64(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d1_fp32(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d2_fp32(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d3_fp32(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+
+// Ghost fill of Q from its interior (every built-in boundary kind).
+cudaError_t launch_fill_bcs(const StageParams& p, int ndim, cudaStream_t s);
+// CFL minimum over every cell of Q (ghosts included) into blk->cfl_min_bits,
+// which the launch first resets.
+cudaError_t launch_cfl_min(const StageParams& p, int ndim, cudaStream_t s);
+// Device-driven loop bookkeeping (see util_kernels.cu).
+cudaError_t launch_clock_init(DeviceBlock* blk, double time, double max_time, double prev_output_time,
+                              double output_delta, double max_cfl, cudaStream_t s);
+cudaError_t launch_clock_advance(DeviceBlock* blk, double* dt_log, int first, cudaStream_t s);
+
+} // namespace mc

@@ -1,0 +1,121 @@
+// Launchers of the stage kernels for one dimension (MC_DIM) and one compute
+// type (MC_REAL). Each stage_d<dim>_<precision>.cu translation unit defines
+// the two macros and includes this file, so the template instantiations of
+// the different dimensions and precisions compile in parallel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "launch.h"
+#include "stage_kernels.cuh"
+
+#ifndef MC_DIM
+#error "MC_DIM must be defined"
+#endif
+#ifndef MC_REAL
+#error "MC_REAL must be defined"
+#endif
+#ifndef MC_LAUNCH_NAME
+#error "MC_LAUNCH_NAME must be defined"
+#endif
+
+namespace mc {
+namespace {
+
+using Real = MC_REAL;
+
+inline int cdiv(long long a, long long b) {
+    return (int)((a + b - 1) / b);
+}
+
+// Raise the dynamic shared-memory limit of a kernel once per process.
+template <class K>
+cudaError_t allow_smem(K kernel, size_t bytes) {
+    if (bytes <= 48 * 1024) {
+        return cudaSuccess;
+    }
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int REC, int LIM, int RS>
+cudaError_t launch_one(const StageParams& p, int pass, cudaStream_t s) {
+#if MC_DIM == 1
+    (void)pass;
+    auto k = stage1d_kernel<REC, LIM, RS, Real>;
+    const size_t sm = smem_bytes<1, REC, Real>(p.nvar);
+    cudaError_t e = allow_smem(k, sm);
+    if (e != cudaSuccess) {
+        return e;
+    }
+    k<<<dim3(cdiv(p.nx, kWarps * kTile)), dim3(kThreads), sm, s>>>(p);
+#elif MC_DIM == 2
+    (void)pass;
+    auto k = stage2d_kernel<2, REC, LIM, RS, Real>;
+    const size_t sm = smem_bytes<2, REC, Real>(p.nvar);
+    cudaError_t e = allow_smem(k, sm);
+    if (e != cudaSuccess) {
+        return e;
+    }
+    k<<<dim3(cdiv(p.nx, kTile), cdiv(p.ny, kTile)), dim3(kThreads), sm, s>>>(p);
+#else
+    if (pass == 0) {
+        auto k = stage2d_kernel<3, REC, LIM, RS, Real>;
+        const size_t sm = smem_bytes<3, REC, Real>(p.nvar);
+        cudaError_t e = allow_smem(k, sm);
+        if (e != cudaSuccess) {
+            return e;
+        }
+        k<<<dim3(cdiv(p.nx, kTile), cdiv(p.ny, kTile), p.nz), dim3(kThreads), sm, s>>>(p);
+    } else {
+        zsweep3d_kernel<REC, LIM, RS, Real>
+            <<<dim3(cdiv(p.nx, kZBlockX), cdiv(p.ny, kZBlockY), cdiv(p.nz, kZChunk)), dim3(kZBlockX, kZBlockY), 0,
+               s>>>(p);
+    }
+#endif
+    return cudaGetLastError();
+}
+
+template <int REC, int LIM>
+cudaError_t by_solver(const StageParams& p, int rs, int pass, cudaStream_t s) {
+    switch (rs) {
+        case kRusanov:
+            return launch_one<REC, LIM, kRusanov>(p, pass, s);
+        case kHll:
+            return launch_one<REC, LIM, kHll>(p, pass, s);
+        default:
+            return launch_one<REC, LIM, kHllc>(p, pass, s);
+    }
+}
+
+} // namespace
+
+// Dispatch on (reconstruction, limiter, solver). The limiter only matters for
+// MUSCL and PPM; FOG and WENO5-Z are limiter-agnostic (Reconstruct.hpp:33-44).
+cudaError_t MC_LAUNCH_NAME(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s) {
+    switch (rec) {
+        case kFog:
+            return by_solver<kFog, kMonotonizedCentral>(p, rs, pass, s);
+        case kMuscl:
+            switch (lim) {
+                case kVanLeer:
+                    return by_solver<kMuscl, kVanLeer>(p, rs, pass, s);
+                case kMonotonizedCentral:
+                    return by_solver<kMuscl, kMonotonizedCentral>(p, rs, pass, s);
+                default:
+                    return by_solver<kMuscl, kMinmod>(p, rs, pass, s);
+            }
+        case kPpm:
+            switch (lim) {
+                case kVanLeer:
+                    return by_solver<kPpm, kVanLeer>(p, rs, pass, s);
+                case kMonotonizedCentral:
+                    return by_solver<kPpm, kMonotonizedCentral>(p, rs, pass, s);
+                default:
+                    return by_solver<kPpm, kMinmod>(p, rs, pass, s);
+            }
+        default:
+            return by_solver<kWeno5z, kMonotonizedCentral>(p, rs, pass, s);
+    }
+}
+
+} // namespace mc

@@ -1,0 +1,587 @@
+// Fused SSPRK stage kernels.
+//
+// One launch performs one stage of the reference's time_step
+// (source/TimeStepping.cpp) for a whole grid:
+//   global_cons_to_prim -> reconstruct / Riemann flux per axis ->
+//   integrate_flux + stage combination -> fill_bcs
+// (source/Hydro.cpp:8-166, source/TimeStepping.cpp:10-35, Boundaries.hpp)
+// without any intermediate array in global memory: the primitive tile, the
+// face states and the fluxes live in shared memory and registers.
+//
+// Work decomposition (1D / 2D, and the x-y part of 3D):
+//   * a CTA owns a tile of TX x TY output cells (TX = TY = 30 in 2D);
+//   * phase 1 loads the tile plus a cross-shaped halo of H cells, converts
+//     to primitives once per cell and stores them in shared memory;
+//   * phase 2 gives one warp per row: lane L reconstructs cell L-1 (cells
+//     -1..30), receives the left state of its face from lane L-1 with a
+//     shuffle, solves the Riemann problem for the face on the left of its
+//     cell, and takes the right face's flux from lane L+1 -- every face is
+//     solved once and every cell is reconstructed once per axis;
+//   * phase 3 does the same along y with one warp per column;
+//   * phase 4 combines the divergence with the stage inputs, writes the new
+//     state, scatters the ghost cells it is the source of, and (last stage)
+//     reduces the CFL minimum and status flags.
+// 3D splits each stage in two launches: the x-y plane pass above writes the
+// x+y divergence per cell, then a z-march kernel (one thread per (x, y)
+// column, a register window along z) adds the z divergence and finishes
+// the stage.
+#pragma once
+
+#include "common.cuh"
+
+namespace mc {
+
+constexpr int kTile = 30;     // output cells per warp-wide row segment
+constexpr int kThreads = 256; // threads per CTA of the tiled kernels
+constexpr int kWarps = kThreads / 32;
+
+// Shared-memory geometry of the tiled kernels.
+template <int NDIM, int REC>
+struct TileGeom {
+    static constexpr int H = halo_of<REC>();
+    static constexpr int TX = kTile;
+    static constexpr int TY = NDIM == 1 ? 1 : kTile;
+    static constexpr int WX = TX + 2 * H;                    // stored columns
+    static constexpr int P = (WX % 2 == 0) ? WX + 1 : WX;    // odd pitch: conflict-free columns
+    static constexpr int WY = NDIM == 1 ? 1 : TY + 2 * H;    // stored rows
+    static constexpr int PY = TX + 1;                        // odd pitch of the y divergence
+};
+
+// Element counts of the per-variable shared arrays (1D uses a different
+// layout: NW segments of TX cells).
+template <int NDIM, int REC>
+__host__ __device__ constexpr int smem_w_per_var() {
+    using G = TileGeom<NDIM, REC>;
+    return NDIM == 1 ? (kWarps * kTile + 2 * G::H) : G::WY * G::P;
+}
+template <int NDIM, int REC>
+__host__ __device__ constexpr int smem_dqx_per_var() {
+    using G = TileGeom<NDIM, REC>;
+    return NDIM == 1 ? 0 : G::TY * G::TX;
+}
+template <int NDIM, int REC>
+__host__ __device__ constexpr int smem_dqy_per_var() {
+    using G = TileGeom<NDIM, REC>;
+    return NDIM == 1 ? 0 : G::TY * G::PY;
+}
+template <int NDIM, int REC, class T>
+__host__ __device__ constexpr size_t smem_bytes(int nvar) {
+    return sizeof(T) * (size_t)nvar *
+           (smem_w_per_var<NDIM, REC>() + smem_dqx_per_var<NDIM, REC>() + smem_dqy_per_var<NDIM, REC>());
+}
+
+__device__ __forceinline__ long long qidx(const StageParams& p, int v, int k, int j, int i) {
+    return (((long long)v * p.zc + k) * p.yc + j) * (long long)p.xc + i;
+}
+
+// Write the new value of interior cell (i, j, k) and every ghost it is the
+// source of; returns the CFL minimum over the written values (last stage) and
+// ORs their status flags into *flags.
+template <int NDIM>
+__device__ __forceinline__ double write_cell(const StageParams& p, int i, int j, int k, double* qn,
+                                             bool want_dt, unsigned* flags) {
+    constexpr int nh = 2 + NDIM;
+    const int nvar = p.nvar;
+    double dtmin = __longlong_as_double(0x7ff0000000000000ll);
+    auto account = [&](const double* q) {
+        if (want_dt) {
+            double w[nh];
+            prim_from_cons<NDIM>(p.gamma, q, w);
+            bool fin = true;
+#pragma unroll
+            for (int v = 0; v < nh; ++v) {
+                fin = fin && isfinite(q[v]);
+            }
+            *flags |= state_flags(w[0], w[nh - 1], fin);
+            const double d = cfl_dt<NDIM>(p.gamma, p.dx, w);
+            dtmin = smin(d, dtmin);
+        }
+    };
+#pragma unroll
+    for (int v = 0; v < kMaxVars; ++v) {
+        if (v < nvar) {
+            p.q_out[qidx(p, v, k, j, i)] = qn[v];
+        }
+    }
+    account(qn);
+    const bool nx_ = near_face(i, p.nx, p.ng);
+    const bool ny_ = NDIM > 1 && near_face(j, p.ny, p.ng);
+    const bool nz_ = NDIM > 2 && near_face(k, p.nz, p.ng);
+    if (!(nx_ || ny_ || nz_)) {
+        return dtmin;
+    }
+    int ix[2 * kMaxGhost + 1], fx[2 * kMaxGhost + 1];
+    int iy[2 * kMaxGhost + 1], fy[2 * kMaxGhost + 1];
+    int iz[2 * kMaxGhost + 1], fz[2 * kMaxGhost + 1];
+    const int cx = axis_targets(i, p.nx, p.ng, p.bc.kind[0], p.bc.kind[1], ix, fx);
+    int cy = 1, cz = 1;
+    iy[0] = j;
+    fy[0] = -1;
+    iz[0] = k;
+    fz[0] = -1;
+    if constexpr (NDIM > 1) {
+        cy = axis_targets(j, p.ny, p.ng, p.bc.kind[2], p.bc.kind[3], iy, fy);
+    }
+    if constexpr (NDIM > 2) {
+        cz = axis_targets(k, p.nz, p.ng, p.bc.kind[4], p.bc.kind[5], iz, fz);
+    }
+    for (int a = 0; a < cx; ++a) {
+        double qa[kMaxVars];
+#pragma unroll
+        for (int v = 0; v < kMaxVars; ++v) {
+            qa[v] = qn[v];
+        }
+        if (fx[a] >= 0) {
+            bc_transform<NDIM>(p.bc, 0, fx[a], nvar, qa);
+        }
+        for (int b = 0; b < cy; ++b) {
+            double qb[kMaxVars];
+#pragma unroll
+            for (int v = 0; v < kMaxVars; ++v) {
+                qb[v] = qa[v];
+            }
+            if (fy[b] >= 0) {
+                bc_transform<NDIM>(p.bc, 1, fy[b], nvar, qb);
+            }
+            for (int c = 0; c < cz; ++c) {
+                if (a == 0 && b == 0 && c == 0) {
+                    continue;
+                }
+                double qc[kMaxVars];
+#pragma unroll
+                for (int v = 0; v < kMaxVars; ++v) {
+                    qc[v] = qb[v];
+                }
+                if (fz[c] >= 0) {
+                    bc_transform<NDIM>(p.bc, 2, fz[c], nvar, qc);
+                }
+#pragma unroll
+                for (int v = 0; v < kMaxVars; ++v) {
+                    if (v < nvar) {
+                        p.q_out[qidx(p, v, iz[c], iy[b], ix[a])] = qc[v];
+                    }
+                }
+                account(qc);
+            }
+        }
+    }
+    return dtmin;
+}
+
+// Load one cell's conserved variables from q_in and store its primitives
+// (tracers divided by rho, source/Hydro.cpp:27-33) into shared memory.
+template <int NDIM, class T>
+__device__ __forceinline__ unsigned load_prim(const StageParams& p, int k, int j, int i, bool inb, T* w_smem,
+                                              int var_stride) {
+    constexpr int nh = 2 + NDIM;
+    double q[nh], w[nh];
+    if (inb) {
+#pragma unroll
+        for (int v = 0; v < nh; ++v) {
+            q[v] = p.q_in[qidx(p, v, k, j, i)];
+        }
+    } else {
+        // outside the array: a benign state that no stored result depends on
+        q[0] = 1.0;
+#pragma unroll
+        for (int v = 1; v < nh - 1; ++v) {
+            q[v] = 0.0;
+        }
+        q[nh - 1] = 1.0;
+    }
+    prim_from_cons<NDIM>(p.gamma, q, w);
+#pragma unroll
+    for (int v = 0; v < nh; ++v) {
+        w_smem[v * var_stride] = T(w[v]);
+    }
+    if (p.ntracer > 0) {
+        const double inv_rho = 1.0 / q[0];
+        for (int t = 0; t < p.ntracer; ++t) {
+            const double qt = inb ? p.q_in[qidx(p, nh + t, k, j, i)] : 0.0;
+            w_smem[(nh + t) * var_stride] = T(qt * inv_rho);
+        }
+    }
+    if (!inb) {
+        return 0u;
+    }
+    bool fin = true;
+#pragma unroll
+    for (int v = 0; v < nh; ++v) {
+        fin = fin && isfinite(q[v]);
+    }
+    return state_flags(w[0], w[nh - 1], fin);
+}
+
+// One warp-wide face sweep along AXIS: lane L reconstructs the cell whose
+// stencil centre is at centre_of(L) (cell L-1 of the segment), solves the
+// face on its left, and returns in d[] the divergence F(left) - F(right) of
+// its cell (meaningful on lanes 1..kTile). `stride` is the distance between
+// neighbouring cells along AXIS in shared memory, `vstride` between variables.
+template <int AXIS, int NDIM, int REC, int LIM, int RS, class T>
+__device__ __forceinline__ void face_sweep(const T* centre, int stride, int vstride, int ntracer, T gamma, T* d,
+                                           T* d_tr) {
+    constexpr int nh = 2 + NDIM;
+    constexpr int S = stencil_half<REC>();
+    T wl[nh], wr[nh];
+#pragma unroll
+    for (int v = 0; v < nh; ++v) {
+        T s[5];
+#pragma unroll
+        for (int o = -S; o <= S; ++o) {
+            s[2 + o] = centre[v * vstride + o * stride];
+        }
+        reconstruct<REC, LIM>(s, wl[v], wr[v]);
+    }
+    T left[nh];
+#pragma unroll
+    for (int v = 0; v < nh; ++v) {
+        left[v] = __shfl_up_sync(0xffffffffu, wr[v], 1);
+    }
+    T f[nh];
+    riemann<RS, AXIS, NDIM>(gamma, left, wl, f);
+#pragma unroll
+    for (int v = 0; v < nh; ++v) {
+        const T fn = __shfl_down_sync(0xffffffffu, f[v], 1);
+        d[v] = f[v] - fn;
+    }
+    // passive tracers: upwinded by the sign of the mass flux (Hydro.cpp:155-162)
+    for (int t = 0; t < ntracer; ++t) {
+        T s[5];
+#pragma unroll
+        for (int o = -S; o <= S; ++o) {
+            s[2 + o] = centre[(nh + t) * vstride + o * stride];
+        }
+        T tl, tr;
+        reconstruct<REC, LIM>(s, tl, tr);
+        const T tleft = __shfl_up_sync(0xffffffffu, tr, 1);
+        const T ft = (f[0] >= T(0)) ? f[0] * tleft : f[0] * tl;
+        const T fn = __shfl_down_sync(0xffffffffu, ft, 1);
+        d_tr[t] = ft - fn;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 1D stage kernel: a CTA owns kWarps segments of kTile cells.
+// ---------------------------------------------------------------------------
+template <int REC, int LIM, int RS, class T>
+__global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
+    if (p.dt_dev && p.blk->done) {
+        return;
+    }
+    maybe_reset_min(p);
+    constexpr int NDIM = 1;
+    constexpr int nh = 3;
+    using G = TileGeom<1, REC>;
+    constexpr int H = G::H;
+    constexpr int WN = kWarps * kTile + 2 * H;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red_d[kWarps];
+    __shared__ unsigned red_u[kWarps];
+    T* W = reinterpret_cast<T*>(smem_raw);
+
+    const int x0 = blockIdx.x * (kWarps * kTile);  // first interior cell of the CTA
+    unsigned flags = 0;
+    for (int it = threadIdx.x; it < WN; it += kThreads) {
+        const int i = p.ng + x0 - H + it;  // array index
+        const bool inb = i >= 0 && i < p.xc;
+        flags |= load_prim<NDIM, T>(p, 0, 0, i, inb, W + it, WN);
+    }
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int cl = warp * kTile + lane - 1;  // cell of this lane, relative to x0
+    T d[nh], d_tr[kMaxVars];
+    face_sweep<0, NDIM, REC, LIM, RS, T>(W + H + cl, 1, WN, p.ntracer, T(p.gamma), d, d_tr);
+
+    const double dt = stage_dt(p);
+    const double dtdx = dt / p.dx;
+    double dtmin = __longlong_as_double(0x7ff0000000000000ll);
+    const int cell = x0 + cl;  // interior index
+    if (lane >= 1 && lane <= kTile && cell < p.nx) {
+        const int i = cell + p.ng;
+        double qn[kMaxVars];
+#pragma unroll
+        for (int v = 0; v < kMaxVars; ++v) {
+            qn[v] = 0.0;
+        }
+        const bool old = combo_reads_old(p.combo);
+#pragma unroll
+        for (int v = 0; v < nh; ++v) {
+            double qu = 0.0;
+            qu += double(d[v]);
+            qu *= dtdx;
+            const long long id = qidx(p, v, 0, 0, i);
+            qn[v] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0 * dt);
+        }
+        for (int t = 0; t < p.ntracer; ++t) {
+            double qu = 0.0;
+            qu += double(d_tr[t]);
+            qu *= dtdx;
+            const long long id = qidx(p, nh + t, 0, 0, i);
+            qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0);
+        }
+        dtmin = write_cell<NDIM>(p, i, 0, 0, qn, p.last != 0, &flags);
+    }
+    block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
+}
+
+// ---------------------------------------------------------------------------
+// 2D stage kernel, and the x-y pass of 3D (NDIM == 3: one z plane per
+// blockIdx.z, writing the x+y divergence instead of finishing the stage).
+// ---------------------------------------------------------------------------
+template <int NDIM, int REC, int LIM, int RS, class T>
+__global__ void __launch_bounds__(kThreads) stage2d_kernel(StageParams p) {
+    if (p.dt_dev && p.blk->done) {
+        return;
+    }
+    maybe_reset_min(p);
+    constexpr int nh = 2 + NDIM;
+    using G = TileGeom<2, REC>;
+    constexpr int H = G::H, TX = G::TX, TY = G::TY, WX = G::WX, P = G::P, WY = G::WY, PY = G::PY;
+    constexpr int WV = WY * P;   // per-variable stride of W
+    constexpr int XV = TY * TX;  // per-variable stride of dQx
+    constexpr int YV = TY * PY;  // per-variable stride of dQy
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* W = reinterpret_cast<T*>(smem_raw);
+    T* DX = W + (size_t)p.nvar * WV;
+    T* DY = DX + (size_t)p.nvar * XV;
+    __shared__ double red_d[kWarps];
+    __shared__ unsigned red_u[kWarps];
+
+    const int x0 = blockIdx.x * TX;
+    const int y0 = blockIdx.y * TY;
+    const int k = NDIM == 3 ? p.ng + blockIdx.z : 0;
+    const int vw = min(TX, p.nx - x0);
+    const int vh = min(TY, p.ny - y0);
+
+    // phase 1: primitives of the tile and its cross-shaped halo
+    unsigned flags = 0;
+    constexpr int core = TY * WX;
+    constexpr int items = core + 2 * H * TX;
+    for (int it = threadIdx.x; it < items; it += kThreads) {
+        int tx, ty;
+        if (it < core) {
+            ty = it / WX;
+            tx = it - ty * WX - H;
+        } else {
+            const int r = it - core;
+            const int hr = r / TX;
+            tx = r - hr * TX;
+            ty = hr < H ? hr - H : TY + hr - H;
+        }
+        const int i = p.ng + x0 + tx;
+        const int j = p.ng + y0 + ty;
+        const bool inb = i >= 0 && i < p.xc && j >= 0 && j < p.yc;
+        flags |= load_prim<NDIM, T>(p, k, j, i, inb, W + (ty + H) * P + (tx + H), WV);
+    }
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const T gamma = T(p.gamma);
+    const int ntr = p.ntracer;
+
+    // phase 2: x faces, one warp per row
+    for (int r = warp; r < vh; r += kWarps) {
+        const int cx = lane - 1;
+        T d[nh], d_tr[kMaxVars];
+        face_sweep<0, NDIM, REC, LIM, RS, T>(W + (r + H) * P + (cx + H), 1, WV, ntr, gamma, d, d_tr);
+        if (lane >= 1 && lane <= TX) {
+#pragma unroll
+            for (int v = 0; v < nh; ++v) {
+                DX[v * XV + r * TX + cx] = d[v];
+            }
+            for (int t = 0; t < ntr; ++t) {
+                DX[(nh + t) * XV + r * TX + cx] = d_tr[t];
+            }
+        }
+    }
+    // phase 3: y faces, one warp per column
+    for (int c = warp; c < vw; c += kWarps) {
+        const int cy = lane - 1;
+        T d[nh], d_tr[kMaxVars];
+        face_sweep<1, NDIM, REC, LIM, RS, T>(W + (cy + H) * P + (c + H), P, WV, ntr, gamma, d, d_tr);
+        if (lane >= 1 && lane <= TY) {
+#pragma unroll
+            for (int v = 0; v < nh; ++v) {
+                DY[v * YV + cy * PY + c] = d[v];
+            }
+            for (int t = 0; t < ntr; ++t) {
+                DY[(nh + t) * YV + cy * PY + c] = d_tr[t];
+            }
+        }
+    }
+    __syncthreads();
+
+    // phase 4: stage update (2D) or x+y divergence (3D)
+    const double dt = stage_dt(p);
+    const double dtdx = dt / p.dx;
+    double dtmin = __longlong_as_double(0x7ff0000000000000ll);
+    for (int it = threadIdx.x; it < TX * TY; it += kThreads) {
+        const int ty = it / TX;
+        const int tx = it - ty * TX;
+        if (tx >= vw || ty >= vh) {
+            continue;
+        }
+        const int i = p.ng + x0 + tx;
+        const int j = p.ng + y0 + ty;
+        if constexpr (NDIM == 3) {
+            const long long cells = (long long)p.nx * p.ny * p.nz;
+            const long long o = ((long long)(k - p.ng) * p.ny + (j - p.ng)) * p.nx + (i - p.ng);
+            for (int v = 0; v < p.nvar; ++v) {
+                double qu = 0.0;
+                qu += double(DX[v * XV + ty * TX + tx]);
+                qu += double(DY[v * YV + ty * PY + tx]);
+                p.dqxy[v * cells + o] = qu;
+            }
+        } else {
+            double qn[kMaxVars];
+#pragma unroll
+            for (int v = 0; v < kMaxVars; ++v) {
+                qn[v] = 0.0;
+            }
+#pragma unroll
+            for (int v = 0; v < kMaxVars; ++v) {
+                if (v < p.nvar) {
+                    double qu = 0.0;
+                    qu += double(DX[v * XV + ty * TX + tx]);
+                    qu += double(DY[v * YV + ty * PY + tx]);
+                    qu *= dtdx;
+                    const double src = (v < nh) ? 0.0 * dt : 0.0;
+                    const long long id = qidx(p, v, 0, j, i);
+                    const double qo = combo_reads_old(p.combo) ? p.q_old[id] : 0.0;
+                    qn[v] = combine(p.combo, qo, p.q_in[id], qu, src);
+                }
+            }
+            dtmin = smin(write_cell<NDIM>(p, i, j, 0, qn, p.last != 0, &flags), dtmin);
+        }
+    }
+    block_publish(dtmin, flags, NDIM != 3 && p.last != 0, p.blk, red_d, red_u);
+}
+
+// ---------------------------------------------------------------------------
+// 3D z pass: one thread per interior (x, y) column, marching along z over a
+// chunk of kZChunk cells with a register window of primitives. Adds the z
+// divergence to the x+y divergence from the plane pass and finishes the
+// stage. No passive tracers.
+// ---------------------------------------------------------------------------
+constexpr int kZChunk = 32;
+constexpr int kZBlockX = 32, kZBlockY = 4;
+
+template <int REC, int LIM, int RS, class T>
+__global__ void __launch_bounds__(kZBlockX* kZBlockY) zsweep3d_kernel(StageParams p) {
+    if (p.dt_dev && p.blk->done) {
+        return;
+    }
+    maybe_reset_min(p);
+    constexpr int NDIM = 3;
+    constexpr int nh = 5;
+    constexpr int S = stencil_half<REC>();
+    constexpr int WN = 2 * S + 1;  // window length
+    __shared__ double red_d[kWarps];
+    __shared__ unsigned red_u[kWarps];
+    const int xi = blockIdx.x * kZBlockX + threadIdx.x;
+    const int yi = blockIdx.y * kZBlockY + threadIdx.y;
+    const int z0 = blockIdx.z * kZChunk;
+    const int z1 = min(z0 + kZChunk, p.nz);
+    const bool active = xi < p.nx && yi < p.ny;
+    const int i = xi + p.ng, j = yi + p.ng;
+    const T gamma = T(p.gamma);
+    const double dt = stage_dt(p);
+    const double dtdx = dt / p.dx;
+    const long long cells = (long long)p.nx * p.ny * p.nz;
+    unsigned flags = 0;
+    double dtmin = __longlong_as_double(0x7ff0000000000000ll);
+
+    if (active) {
+        auto load_w = [&](int zc_interior, T* w) {
+            double q[nh], wd[nh];
+            const int kk = zc_interior + p.ng;
+#pragma unroll
+            for (int v = 0; v < nh; ++v) {
+                q[v] = p.q_in[qidx(p, v, kk, j, i)];
+            }
+            prim_from_cons<NDIM>(p.gamma, q, wd);
+            bool fin = true;
+#pragma unroll
+            for (int v = 0; v < nh; ++v) {
+                fin = fin && isfinite(q[v]);
+                w[v] = T(wd[v]);
+            }
+            return state_flags(wd[0], wd[nh - 1], fin);
+        };
+        // window[o][v] holds the primitives of cell (zc - S + o) where zc is
+        // the cell being reconstructed
+        T win[WN][nh];
+        // cells z0-1-S .. z0-1+S for the reconstruction of cell z0-1
+#pragma unroll
+        for (int o = 0; o < WN; ++o) {
+            flags |= load_w(z0 - 1 - S + o, win[o]);
+        }
+        auto recon_window = [&](T* rl, T* rr) {
+#pragma unroll
+            for (int v = 0; v < nh; ++v) {
+                T s[5];
+#pragma unroll
+                for (int o = 0; o < WN; ++o) {
+                    s[2 - S + o] = win[o][v];
+                }
+                reconstruct<REC, LIM>(s, rl[v], rr[v]);
+            }
+        };
+        auto shift_in = [&](int zc_interior) {
+#pragma unroll
+            for (int o = 0; o < WN - 1; ++o) {
+#pragma unroll
+                for (int v = 0; v < nh; ++v) {
+                    win[o][v] = win[o + 1][v];
+                }
+            }
+            flags |= load_w(zc_interior, win[WN - 1]);
+        };
+        T rr_prev[nh], rl_cur[nh], rr_cur[nh], f_prev[nh], f_cur[nh];
+        {
+            T rl_tmp[nh];
+            recon_window(rl_tmp, rr_prev);  // cell z0-1
+        }
+        shift_in(z0 + S);
+        recon_window(rl_cur, rr_cur);  // cell z0
+        riemann<RS, 2, NDIM>(gamma, rr_prev, rl_cur, f_prev);  // face z0 - 1/2
+#pragma unroll
+        for (int v = 0; v < nh; ++v) {
+            rr_prev[v] = rr_cur[v];
+        }
+        for (int z = z0; z < z1; ++z) {
+            shift_in(z + 1 + S);
+            recon_window(rl_cur, rr_cur);  // cell z+1
+            riemann<RS, 2, NDIM>(gamma, rr_prev, rl_cur, f_cur);  // face z + 1/2
+            const int kk = z + p.ng;
+            const long long o = ((long long)z * p.ny + yi) * p.nx + xi;
+            double qn[kMaxVars];
+#pragma unroll
+            for (int v = 0; v < kMaxVars; ++v) {
+                qn[v] = 0.0;
+            }
+#pragma unroll
+            for (int v = 0; v < nh; ++v) {
+                double qu = p.dqxy[v * cells + o];
+                qu += double(f_prev[v] - f_cur[v]);
+                qu *= dtdx;
+                const double src = 0.0 * dt;
+                const long long id = qidx(p, v, kk, j, i);
+                const double qo = combo_reads_old(p.combo) ? p.q_old[id] : 0.0;
+                qn[v] = combine(p.combo, qo, p.q_in[id], qu, src);
+            }
+            dtmin = smin(write_cell<NDIM>(p, i, j, kk, qn, p.last != 0, &flags), dtmin);
+#pragma unroll
+            for (int v = 0; v < nh; ++v) {
+                f_prev[v] = f_cur[v];
+                rr_prev[v] = rr_cur[v];
+            }
+        }
+    }
+    block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
+}
+
+} // namespace mc

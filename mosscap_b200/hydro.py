@@ -1,0 +1,186 @@
+"""Host-side mirror of the hydro part of Mosscap's ``Simulation``.
+
+:class:`HydroSim` holds the conserved state ``Q`` on the GPU (a float64 torch
+tensor in the reference layout ``[var][zc][yc][xc]``) together with the clock
+of ``Simulation``/``OutputConfig``, and exposes the reference's hooks with
+their names and meaning:
+
+=====================  ==========================================  =========================
+reference              here                                        C ABI
+=====================  ==========================================  =========================
+``fill_bcs(sim)``      :meth:`HydroSim.fill_bcs`                   ``mc_fill_bcs``
+``sim.compute_dt``     :meth:`HydroSim.compute_dt` (with clamp)    ``mc_compute_dt``
+``sim.time_step``      :meth:`HydroSim.time_step` (``time += dt``) ``mc_time_step``
+main loop              :meth:`HydroSim.run` / :meth:`advance`      ``mc_advance``
+=====================  ==========================================  =========================
+
+(``source/Boundaries.hpp:132-149``, ``source/Hydro.cpp:345``,
+``source/TimeStepping.cpp:39-308``, ``source/main.cpp:54-72``.)
+
+torch provides device memory and streams only; every computation is a kernel
+of ``libmosscap_b200.so``.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import capi
+from .problems import Problem
+
+
+class HydroSim:
+    def __init__(self, problem: Problem, precision: str = "fp64", device: Optional[torch.device] = None,
+                 Q: Optional[np.ndarray] = None):
+        self.lib = capi.load()
+        self.problem = problem
+        self.device = torch.device(device or "cuda")
+        p = problem
+        shape = p.shape
+        g = capi.McGrid()
+        g.num_dim = p.num_dim
+        g.zc, g.yc, g.xc = shape[1], shape[2], shape[3]
+        g.ng = p.ng
+        g.num_tracers = p.num_tracers
+        g.dx = p.dx
+        for a in range(3):
+            g.loc[a] = p.loc[a]
+        for f in range(6):
+            g.bc[f] = capi.BOUNDARY[p.bc[f]]
+        if p.bc_const is not None:
+            bcc = np.asarray(p.bc_const, dtype=np.float64).reshape(6, 5)
+            for f in range(6):
+                for v in range(5):
+                    g.bc_const[f][v] = bcc[f, v]
+        s = capi.McScheme()
+        s.reconstruction = capi.RECON[p.reconstruction]
+        s.slope_limiter = capi.LIMITER[p.slope_limiter]
+        s.riemann_solver = capi.RIEMANN[p.riemann_solver]
+        s.time_stepper = capi.STEPPER[p.time_stepper]
+        s.precision = capi.PRECISION[precision]
+        s.gamma = p.gamma
+        s.max_cfl = p.max_cfl
+        self._grid, self._scheme = g, s
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            capi.check(self.lib.mc_create(ctypes.byref(g), ctypes.byref(s), ctypes.byref(h)), "mc_create")
+        self.ctx = h
+        q = Q if Q is not None else p.Q
+        if q is None:
+            raise ValueError("no initial state")
+        self.Q = torch.from_numpy(np.ascontiguousarray(q, dtype=np.float64)).to(self.device)
+        assert tuple(self.Q.shape) == tuple(shape)
+        # Simulation::time and the OutputConfig clock; setup_sim writes the
+        # initial conditions at time 0 (source/SetupModules.hpp:258-259)
+        self.time = 0.0
+        self.max_time = p.max_time
+        self.output_delta = p.output_delta
+        self.prev_output_time = 0.0
+        self.current_step = 0
+
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self.lib.mc_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- plumbing ---------------------------------------------------------
+    def _stream(self) -> ctypes.c_void_p:
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def _qptr(self, q: Optional[torch.Tensor] = None) -> ctypes.c_void_p:
+        q = self.Q if q is None else q
+        assert q.is_cuda and q.dtype == torch.float64 and q.is_contiguous()
+        return ctypes.c_void_p(q.data_ptr())
+
+    def _clock(self) -> capi.McClock:
+        c = capi.McClock()
+        c.time, c.max_time = self.time, self.max_time
+        c.prev_output_time, c.output_delta = self.prev_output_time, self.output_delta
+        return c
+
+    # ---- the reference's hooks ----------------------------------------------
+    def fill_bcs(self) -> None:
+        capi.check(self.lib.mc_fill_bcs(self.ctx, self._qptr(), self._stream()), "mc_fill_bcs")
+
+    def compute_dt(self, clamp: bool = True) -> float:
+        dt = ctypes.c_double()
+        clk = self._clock()
+        capi.check(self.lib.mc_compute_dt(self.ctx, self._qptr(), ctypes.byref(clk) if clamp else None,
+                                          ctypes.byref(dt), self._stream()), "mc_compute_dt")
+        return dt.value
+
+    def time_step(self, dt: float) -> None:
+        capi.check(self.lib.mc_time_step(self.ctx, self._qptr(), float(dt), self._stream()), "mc_time_step")
+        self.time += dt
+        self.current_step += 1
+
+    def last_cfl_min(self) -> float:
+        v = ctypes.c_double()
+        capi.check(self.lib.mc_last_cfl_min(self.ctx, ctypes.byref(v), self._stream()), "mc_last_cfl_min")
+        return v.value
+
+    def status(self) -> int:
+        f = ctypes.c_uint32()
+        capi.check(self.lib.mc_get_status(self.ctx, ctypes.byref(f), self._stream()), "mc_get_status")
+        return f.value
+
+    def profile_stages(self, enable: bool) -> None:
+        capi.check(self.lib.mc_profile_stages(self.ctx, int(bool(enable))), "mc_profile_stages")
+
+    def stage_time(self, kind: int = 0):
+        """(summed ms, launches) of the stage kernels recorded since
+        profile_stages(True)."""
+        ms, n = ctypes.c_double(), ctypes.c_int64()
+        capi.check(self.lib.mc_stage_time(self.ctx, int(kind), ctypes.byref(ms), ctypes.byref(n)), "mc_stage_time")
+        return ms.value, n.value
+
+    def launch_count(self) -> int:
+        return int(self.lib.mc_launch_count(self.ctx))
+
+    # ---- main loop --------------------------------------------------------
+    def advance(self, max_steps: int, log_dt: bool = True) -> np.ndarray:
+        """Device-driven loop (mc_advance); stops after max_steps, at max_time
+        or after a step that makes an output due. Returns the dt of each step."""
+        clk = self._clock()
+        done = ctypes.c_int64()
+        log = np.zeros(max(int(max_steps), 1), dtype=np.float64)
+        capi.check(self.lib.mc_advance(self.ctx, self._qptr(), ctypes.byref(clk), int(max_steps),
+                                       ctypes.byref(done),
+                                       log.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if log_dt else None,
+                                       self._stream()), "mc_advance")
+        self.time = clk.time
+        self.prev_output_time = clk.prev_output_time
+        self.current_step += done.value
+        return log[:done.value].copy()
+
+    def run(self, max_steps: int = 1 << 62, device_loop: bool = True) -> np.ndarray:
+        """The main loop of source/main.cpp:54-72 (outputs only move the clock)."""
+        dts = []
+        n = 0
+        while self.time < self.max_time and n < max_steps:
+            if device_loop:
+                d = self.advance(max_steps - n)
+                dts.extend(d.tolist())
+                n += len(d)
+                if len(d) == 0:
+                    break
+            else:
+                dt = self.compute_dt()
+                self.time_step(dt)
+                dts.append(dt)
+                n += 1
+                if self.time >= self.prev_output_time + self.output_delta:
+                    self.prev_output_time = self.time
+        return np.asarray(dts)
+
+    def get_Q(self) -> np.ndarray:
+        return self.Q.detach().cpu().numpy()

@@ -145,11 +145,16 @@ def kelvin_helmholtz_2d(n: int = 2048, ng: int = 3, seed: int = 0, noise: float 
     return p
 
 
-def sedov_3d(n: int = 512, ng: int = 3, e_blast: float = 1.0) -> Problem:
+def sedov_3d(n: int = 512, ng: int = 3, e_blast: float = 1.0, max_cfl: float = 0.8 / 3.0) -> Problem:
     """Sedov-style blast on [-1,1]^3: rho = 1, ambient p = 1e-5, gamma = 1.4;
     energy ``e_blast`` deposited uniformly as internal energy in the cells whose
-    centre lies within r < 3 dx. PPM (MC limiter) + HLL, SSPRK3, CFL 0.8,
-    zero-gradient boundaries, to t = 0.05."""
+    centre lies within r < 3 dx. PPM (MC limiter) + HLL, SSPRK3, zero-gradient
+    boundaries, to t = 0.05.
+
+    The CFL number defaults to 0.8 / 3: the reference's CFL bound is
+    per direction (source/Hydro.cpp:192-206) while its 3D update is unsplit,
+    and at 0.8 the reference itself produces negative pressures in the first
+    step and non-finite values from then on at every resolution >= 32^3."""
     dx = 2.0 / n
     c = cell_centres(3, n, ng, dx, -1.0)
     Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
@@ -164,7 +169,7 @@ def sedov_3d(n: int = 512, ng: int = 3, e_blast: float = 1.0) -> Problem:
     w[4] = np.where(hot, 1e-5 + (gamma - 1.0) * de, 1e-5)
     p = Problem("sedov_3d", 3, n, n, n, ng=ng, dx=dx, loc=(-1.0, -1.0, -1.0),
                 bc=("zerograd",) * 6, reconstruction="ppm", slope_limiter="monotonizedcentral",
-                riemann_solver="hll", time_stepper="ssprk3", gamma=gamma, max_cfl=0.8,
+                riemann_solver="hll", time_stepper="ssprk3", gamma=gamma, max_cfl=max_cfl,
                 max_time=0.05, output_delta=0.05)
     p.Q = prim_to_cons(3, gamma, w)
     return p
