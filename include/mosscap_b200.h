@@ -191,6 +191,28 @@ mc_status mc_get_status(mc_ctx* ctx, uint32_t* flags, void* stream);
 mc_status mc_profile_stages(mc_ctx* ctx, int32_t enable);
 mc_status mc_stage_time(mc_ctx* ctx, int32_t kind, double* total_ms, int64_t* launches);
 
+/* One SSPRK step in place on Q, like mc_time_step, without a context and
+ * without allocating any device memory. No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: a code whose device memory is
+ * owned by a pool allocator sized at start-up (Mosscap itself allocates
+ * through a YAKL/Kokkos pool), or one that must not call cudaMalloc/cudaFree
+ * mid-run because those calls synchronise the device. The stage buffers
+ * come from one static device array of 16 MiB that every GPU loading the
+ * library holds until the process exits; a problem needs
+ * 2 x (2+num_dim+num_tracers) x xc x yc x zc doubles (plus
+ * (2+num_dim) x nx x ny x nz in 3D) and is rejected with
+ * MC_ERR_OUT_OF_MEMORY when that exceeds 16 MiB (a 4-variable 2D grid with
+ * 3 ghosts fits up to 506 x 506 interior cells). All faces must be built-in kinds
+ * (no user hook without a context). The first call on a device looks up the
+ * array's device address with that device current; make that first call
+ * before any stream capture. All calls share the array and its contents
+ * persist between calls: calls whose work overlaps on the GPU race and must
+ * not be issued. The CFL minimum and status flags of the call go to a block
+ * shared by all such calls and are not reported. */
+mc_status mc_time_step_noalloc(const mc_grid* grid, const mc_scheme* scheme, double* Q, double dt,
+                               void* stream);
+
 /* Number of kernel launches issued by this context since it was created. */
 int64_t mc_launch_count(const mc_ctx* ctx);
 

@@ -109,6 +109,8 @@ def load() -> ctypes.CDLL:
     lib.mc_profile_stages.restype = i32
     lib.mc_stage_time.argtypes = [vp, i32, P(d), P(i64)]
     lib.mc_stage_time.restype = i32
+    lib.mc_time_step_noalloc.argtypes = [P(McGrid), P(McScheme), vp, d, vp]
+    lib.mc_time_step_noalloc.restype = i32
     lib.mc_launch_count.argtypes = [vp]
     lib.mc_launch_count.restype = i64
     if lib.mc_abi_version() != 1:

@@ -212,6 +212,12 @@ mc_status check_user_bc(const mc_ctx* c) {
 
 } // namespace
 
+namespace mc {
+void set_last_error(const char* msg) {
+    g_error = msg;
+}
+} // namespace mc
+
 extern "C" {
 
 int32_t mc_abi_version(void) {

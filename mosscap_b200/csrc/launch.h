@@ -26,4 +26,7 @@ cudaError_t launch_clock_init(DeviceBlock* blk, double time, double max_time, do
                               double output_delta, double max_cfl, cudaStream_t s);
 cudaError_t launch_clock_advance(DeviceBlock* blk, double* dt_log, int first, cudaStream_t s);
 
+// Record the message mc_last_error returns on this thread (capi.cu).
+void set_last_error(const char* msg);
+
 } // namespace mc
