@@ -191,6 +191,49 @@ mc_status mc_get_status(mc_ctx* ctx, uint32_t* flags, void* stream);
 mc_status mc_profile_stages(mc_ctx* ctx, int32_t enable);
 mc_status mc_stage_time(mc_ctx* ctx, int32_t kind, double* total_ms, int64_t* launches);
 
+/* ---- Batches of independent problems ---------------------------------------
+ *
+ * Thousands of independent 1D / 2D problems of uneven size advance together:
+ * every step of the whole batch is one persistent kernel launch per SSPRK
+ * stage (all problems' tiles in one work list) plus one clock launch, and the
+ * step is replayed from a captured CUDA graph. Each problem runs the
+ * reference's main loop on its own (source/main.cpp:54-72): its own CFL dt,
+ * clamped to its own output times and max_time; outputs only advance its
+ * clock (prev_output_time = time); a problem that reaches max_time stops.
+ * No counterpart as such in the reference (which runs one problem). */
+typedef struct mc_batch mc_batch;
+
+typedef struct {
+    mc_grid grid;     /* num_dim 1 or 2, num_tracers 0, built-in boundary kinds except constant */
+    int64_t offset;   /* offset in doubles of this problem's Q inside the caller's pool */
+    double max_cfl;   /* this problem's CFL number */
+    mc_clock clock;   /* initial clock */
+} mc_batch_problem;
+
+/* The scheme (reconstruction, limiter, solver, stepper, precision, gamma) is
+ * shared; scheme->max_cfl is ignored in favour of each problem's. pool_doubles
+ * is the size of the caller's pool; the batch allocates two more of that size
+ * for its stage buffers. */
+mc_status mc_batch_create(const mc_batch_problem* problems, int32_t n, const mc_scheme* scheme,
+                          int64_t pool_doubles, mc_batch** out);
+mc_status mc_batch_destroy(mc_batch* batch);
+/* Fill every problem's ghost cells (fill_bcs per problem). */
+mc_status mc_batch_fill_bcs(mc_batch* batch, double* pool, void* stream);
+/* Autotuner: times the stage kernel on this pool for every candidate
+ * schedule (persistent grid size, static or dynamic work distribution, 1D
+ * segments per warp task) with CUDA events and keeps the fastest. Leaves the
+ * pool unchanged. Waits for the stream. */
+mc_status mc_batch_tune(mc_batch* batch, double* pool, void* stream);
+/* Up to `steps` steps of every unfinished problem, each with its own dt, on
+ * the device (graph replay). The first call computes every problem's first
+ * dt from its state. */
+mc_status mc_batch_advance(mc_batch* batch, double* pool, int64_t steps, void* stream);
+/* Per-problem clocks, steps taken and MC_FLAG_* status (NULL to skip any).
+ * Waits for the stream. */
+mc_status mc_batch_clocks(mc_batch* batch, mc_clock* clocks, int64_t* steps, uint32_t* status, void* stream);
+/* The schedule in use: grid size in CTAs, 1 if dynamic, 1D segments per warp task. */
+mc_status mc_batch_schedule(const mc_batch* batch, int32_t* grid, int32_t* dynamic, int32_t* segs_per_task);
+
 /* One SSPRK step in place on Q, like mc_time_step, without a context and
  * without allocating any device memory. No counterpart in the reference.
  *

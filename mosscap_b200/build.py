@@ -4,7 +4,8 @@ Every translation unit is compiled by nvcc with
 ``-gencode arch=compute_100a,code=sm_100a -O3 -lineinfo``. The FP64 stage
 kernels and the utility kernels are compiled with ``-fmad=false`` so that no
 multiply-add is contracted: their results are bit-identical to the
-reference's CPU build. The FP32-form kernels keep contraction on.
+reference's CPU build. The FP32-form kernels use ``--use_fast_math``
+(contraction, approximate FP32 division and square root).
 
 Objects go to ``mosscap_b200/_build`` and are rebuilt when any source or
 header is newer. Run ``python -m mosscap_b200.build``.
@@ -38,7 +39,9 @@ def nvcc() -> str:
 def _flags_for(src: str) -> list:
     name = os.path.basename(src)
     exact = "_fp32" not in name
-    return ["-fmad=false"] if exact else ["-fmad=true"]
+    # the FP32 compute form is not bit-exact by design: approximate FP32
+    # division / square root and contraction (FP64 division stays IEEE)
+    return ["-fmad=false"] if exact else ["--use_fast_math"]
 
 
 def _headers_mtime() -> float:

@@ -106,11 +106,42 @@ __device__ __forceinline__ void cons_from_prim(T gamma, const T* w, T* q) {
     q[1 + NDIM] = e_int + e_kin;
 }
 
-// prim_to_flux along AXIS                                          Eos.hpp:101-131
-template <int AXIS, int NDIM, class T>
-__device__ __forceinline__ void flux_from_prim(T gamma, const T* w, T* f) {
-    constexpr int iv = 1 + AXIS;
-    const T mass_flux = w[0] * w[iv];
+// Component 1 + axis of a small register array, for an axis that is
+// uniform across the warp: the array stays in registers because every
+// access below uses a compile-time index.
+template <int NDIM, class T>
+__device__ __forceinline__ T along(const T* a, int axis) {
+    T r = a[1];
+    if constexpr (NDIM > 1) {
+        if (axis == 1) {
+            r = a[2];
+        }
+    }
+    if constexpr (NDIM > 2) {
+        if (axis == 2) {
+            r = a[3];
+        }
+    }
+    return r;
+}
+
+// a[1 + axis] += x
+template <int NDIM, class T>
+__device__ __forceinline__ void add_along(T* a, int axis, T x) {
+    if (axis == 0) {
+        a[1] += x;
+    } else if (NDIM > 1 && axis == 1) {
+        a[NDIM > 1 ? 2 : 1] += x;
+    } else if (NDIM > 2) {
+        a[NDIM > 2 ? 3 : 1] += x;
+    }
+}
+
+// prim_to_flux along `axis` (warp-uniform)                         Eos.hpp:101-131
+template <int NDIM, class T>
+__device__ __forceinline__ void flux_from_prim(T gamma, int axis, const T* w, T* f) {
+    const T vn = along<NDIM>(w, axis);
+    const T mass_flux = w[0] * vn;
     T e_kin = T(0);
     f[0] = mass_flux;
     f[1] = mass_flux * w[1];
@@ -124,9 +155,9 @@ __device__ __forceinline__ void flux_from_prim(T gamma, const T* w, T* f) {
         e_kin += sq(w[3]);
     }
     e_kin *= T(0.5) * w[0];
-    f[iv] += w[1 + NDIM];
+    add_along<NDIM>(f, axis, w[1 + NDIM]);
     const T e_tot = w[1 + NDIM] / (gamma - T(1)) + e_kin;
-    f[1 + NDIM] = (e_tot + w[1 + NDIM]) * w[iv];
+    f[1 + NDIM] = (e_tot + w[1 + NDIM]) * vn;
 }
 
 // CFL time-step bound of one cell from its primitives (dt_reducer,
@@ -230,22 +261,27 @@ __device__ __forceinline__ void reconstruct(const T* s, T& wl, T& wr) {
 
 // ---- Riemann solvers (source/Riemann.hpp), hydro variables only ---------------
 
-template <int RS, int AXIS, int NDIM, class T>
-__device__ __forceinline__ void riemann(T gamma, const T* wL, const T* wR, T* flux) {
+// Interface flux along `axis` (warp-uniform). gfac = (gamma + 1) / (2 gamma),
+// the HLLC shock-factor coefficient, computed once by the caller with that
+// same expression (the reference evaluates it per interface; the value is
+// identical).
+template <int RS, int NDIM, class T>
+__device__ __forceinline__ void riemann(T gamma, T gfac, int axis, const T* wL, const T* wR, T* flux) {
     constexpr int nh = 2 + NDIM;
-    constexpr int iv = 1 + AXIS;
     constexpr int ie = 1 + NDIM;
     const T tiny = T(1e-20);
     T qL[nh], qR[nh], fL[nh], fR[nh];
+    const T vL = along<NDIM>(wL, axis);
+    const T vR = along<NDIM>(wR, axis);
     if constexpr (RS == kRusanov) {
         // local Lax-Friedrichs with the mean of both signal speeds   Riemann.hpp:22-46
         cons_from_prim<NDIM>(gamma, wL, qL);
         cons_from_prim<NDIM>(gamma, wR, qR);
-        flux_from_prim<AXIS, NDIM>(gamma, wL, fL);
-        flux_from_prim<AXIS, NDIM>(gamma, wR, fR);
+        flux_from_prim<NDIM>(gamma, axis, wL, fL);
+        flux_from_prim<NDIM>(gamma, axis, wR, fR);
         const T csL = sound_speed<NDIM>(gamma, wL);
         const T csR = sound_speed<NDIM>(gamma, wR);
-        const T max_c = T(0.5) * (csL + fabs(wL[iv]) + csR + fabs(wR[iv]));
+        const T max_c = T(0.5) * (csL + fabs(vL) + csR + fabs(vR));
 #pragma unroll
         for (int i = 0; i < nh; ++i) {
             flux[i] = T(0.5) * (fL[i] + fR[i] - max_c * (qR[i] - qL[i]));
@@ -255,13 +291,13 @@ __device__ __forceinline__ void riemann(T gamma, const T* wL, const T* wR, T* fl
         // pairs wL's velocity with csR                               Riemann.hpp:48-73
         const T csL = sound_speed<NDIM>(gamma, wL);
         const T csR = sound_speed<NDIM>(gamma, wR);
-        const T sL = smin(-tiny, smin(wL[iv] - csL, wR[iv] - csR));
-        const T sR = smax(-tiny, smax(wL[iv] + csL, wL[iv] + csR));
+        const T sL = smin(-tiny, smin(vL - csL, vR - csR));
+        const T sR = smax(-tiny, smax(vL + csL, vL + csR));
         const T sM = T(1) / (sR - sL);
         cons_from_prim<NDIM>(gamma, wL, qL);
         cons_from_prim<NDIM>(gamma, wR, qR);
-        flux_from_prim<AXIS, NDIM>(gamma, wL, fL);
-        flux_from_prim<AXIS, NDIM>(gamma, wR, fR);
+        flux_from_prim<NDIM>(gamma, axis, wL, fL);
+        flux_from_prim<NDIM>(gamma, axis, wR, fR);
 #pragma unroll
         for (int i = 0; i < nh; ++i) {
             flux[i] = sM * (sR * fL[i] - sL * fR[i] + sR * sL * (qR[i] - qL[i]));
@@ -278,25 +314,23 @@ __device__ __forceinline__ void riemann(T gamma, const T* wL, const T* wR, T* fl
         const T pR = wR[ie];
         const T rho_avg = T(0.5) * (wL[0] + wR[0]);
         const T cs_avg = T(0.5) * (csL + csR);
-        const T p_mid = T(0.5) * (pL + pR + (wL[iv] - wR[iv]) * rho_avg * cs_avg);
-        const T cLstar =
-            (p_mid <= pL) ? T(1) : sqrt(T(1) + (gamma + T(1)) / (T(2) * gamma) * (p_mid / pL - T(1)));
-        const T cRstar =
-            (p_mid <= pR) ? T(1) : sqrt(T(1) + (gamma + T(1)) / (T(2) * gamma) * (p_mid / pR - T(1)));
-        const T aL = wL[iv] - csL * cLstar;
-        const T aR = wR[iv] + csR * cRstar;
+        const T p_mid = T(0.5) * (pL + pR + (vL - vR) * rho_avg * cs_avg);
+        const T cLstar = (p_mid <= pL) ? T(1) : sqrt(T(1) + gfac * (p_mid / pL - T(1)));
+        const T cRstar = (p_mid <= pR) ? T(1) : sqrt(T(1) + gfac * (p_mid / pR - T(1)));
+        const T aL = vL - csL * cLstar;
+        const T aR = vR + csR * cRstar;
         const T bM = smin(-tiny, aL);
         const T bP = smax(tiny, aR);
-        T vxL = wL[iv] - aL;
-        T vxR = wR[iv] - aR;
-        const T tL = pL + vxL * qL[iv];
-        const T tR = pR + vxR * qR[iv];
+        T vxL = vL - aL;
+        T vxR = vR - aR;
+        const T tL = pL + vxL * along<NDIM>(qL, axis);
+        const T tR = pR + vxR * along<NDIM>(qR, axis);
         const T mL = wL[0] * vxL;
         const T mR = -(wR[0] * vxR);
         const T aM = (tL - tR) / (mL + mR);
         const T cp = smax((mL * tR + mR * tL) / (mL + mR), T(0));
-        vxL = wL[iv] - bM;
-        vxR = wR[iv] - bP;
+        vxL = vL - bM;
+        vxR = vR - bP;
         const T mfL = wL[0] * vxL;
         const T mfR = wR[0] * vxR;
         fL[0] = mfL;
@@ -306,10 +340,10 @@ __device__ __forceinline__ void riemann(T gamma, const T* wL, const T* wR, T* fl
             fL[d] = mfL * wL[d];
             fR[d] = mfR * wR[d];
         }
-        fL[iv] += pL;
-        fR[iv] += pR;
-        fL[ie] = qL[ie] * vxL + pL * wL[iv];
-        fR[ie] = qR[ie] * vxR + pR * wR[iv];
+        add_along<NDIM>(fL, axis, pL);
+        add_along<NDIM>(fR, axis, pR);
+        fL[ie] = qL[ie] * vxL + pL * vL;
+        fR[ie] = qR[ie] * vxR + pR * vR;
         T sL, sR, sM;
         if (aM >= T(0)) {
             sL = aM / (aM - bM);
@@ -324,7 +358,7 @@ __device__ __forceinline__ void riemann(T gamma, const T* wL, const T* wR, T* fl
         for (int i = 0; i < nh; ++i) {
             flux[i] = sL * fL[i] + sR * fR[i];
         }
-        flux[iv] += sM * cp;
+        add_along<NDIM>(flux, axis, sM * cp);
         flux[ie] += sM * cp * aM;
     }
 }

@@ -12,15 +12,16 @@
 //   * a CTA owns a tile of TX x TY output cells (TX = TY = 30 in 2D);
 //   * phase 1 loads the tile plus a cross-shaped halo of H cells, converts
 //     to primitives once per cell and stores them in shared memory;
-//   * phase 2 gives one warp per row: lane L reconstructs cell L-1 (cells
-//     -1..30), receives the left state of its face from lane L-1 with a
-//     shuffle, solves the Riemann problem for the face on the left of its
-//     cell, and takes the right face's flux from lane L+1 -- every face is
-//     solved once and every cell is reconstructed once per axis;
-//   * phase 3 does the same along y with one warp per column;
-//   * phase 4 combines the divergence with the stage inputs, writes the new
-//     state, scatters the ghost cells it is the source of, and (last stage)
-//     reduces the CFL minimum and status flags.
+//   * a y sweep gives one warp per column: lane L reconstructs cell L-1
+//     (cells -1..30), receives the left state of its face from lane L-1 with
+//     a shuffle, solves the Riemann problem for the face below its cell, and
+//     takes the next face's flux from lane L+1 -- every face is solved once
+//     and every cell is reconstructed once per axis; the y divergence goes to
+//     shared memory;
+//   * an x sweep does the same with one warp per row, and the lane of each
+//     cell then combines both divergences with the stage inputs, writes the
+//     new state, scatters the ghost cells it is the source of, and (last
+//     stage) reduces the CFL minimum and status flags.
 // 3D splits each stage in two launches: the x-y plane pass above writes the
 // x+y divergence per cell, then a z-march kernel (one thread per (x, y)
 // column, a register window along z) adds the z divergence and finishes
@@ -34,6 +35,12 @@ namespace mc {
 constexpr int kTile = 30;     // output cells per warp-wide row segment
 constexpr int kThreads = 256; // threads per CTA of the tiled kernels
 constexpr int kWarps = kThreads / 32;
+// CTAs per SM the 2D / plane kernel is compiled for. FP64: three (80
+// registers a thread); with the x divergence kept in registers its shared
+// memory (72 KB for four variables) allows three. FP32 compute form: four
+// (64 registers; measured faster than three despite a few spills).
+constexpr int kMinBlocks2d = 3;
+constexpr int kMinBlocks2dF32 = 4;
 
 // Shared-memory geometry of the tiled kernels.
 template <int NDIM, int REC>
@@ -55,19 +62,13 @@ __host__ __device__ constexpr int smem_w_per_var() {
     return NDIM == 1 ? (kWarps * kTile + 2 * G::H) : G::WY * G::P;
 }
 template <int NDIM, int REC>
-__host__ __device__ constexpr int smem_dqx_per_var() {
-    using G = TileGeom<NDIM, REC>;
-    return NDIM == 1 ? 0 : G::TY * G::TX;
-}
-template <int NDIM, int REC>
 __host__ __device__ constexpr int smem_dqy_per_var() {
     using G = TileGeom<NDIM, REC>;
     return NDIM == 1 ? 0 : G::TY * G::PY;
 }
 template <int NDIM, int REC, class T>
 __host__ __device__ constexpr size_t smem_bytes(int nvar) {
-    return sizeof(T) * (size_t)nvar *
-           (smem_w_per_var<NDIM, REC>() + smem_dqx_per_var<NDIM, REC>() + smem_dqy_per_var<NDIM, REC>());
+    return sizeof(T) * (size_t)nvar * (smem_w_per_var<NDIM, REC>() + smem_dqy_per_var<NDIM, REC>());
 }
 
 __device__ __forceinline__ long long qidx(const StageParams& p, int v, int k, int j, int i) {
@@ -212,14 +213,16 @@ __device__ __forceinline__ unsigned load_prim(const StageParams& p, int k, int j
     return state_flags(w[0], w[nh - 1], fin);
 }
 
-// One warp-wide face sweep along AXIS: lane L reconstructs the cell whose
-// stencil centre is at centre_of(L) (cell L-1 of the segment), solves the
-// face on its left, and returns in d[] the divergence F(left) - F(right) of
-// its cell (meaningful on lanes 1..kTile). `stride` is the distance between
-// neighbouring cells along AXIS in shared memory, `vstride` between variables.
-template <int AXIS, int NDIM, int REC, int LIM, int RS, class T>
-__device__ __forceinline__ void face_sweep(const T* centre, int stride, int vstride, int ntracer, T gamma, T* d,
-                                           T* d_tr) {
+// One warp-wide face sweep along `axis` (warp-uniform): lane L reconstructs
+// the cell whose stencil centre is `centre` (cell L-1 of the segment), solves
+// the face on its left, and returns in d[] the divergence F(left) - F(right)
+// of its cell (meaningful on lanes 1..kTile). `stride` is the distance between
+// neighbouring cells along the axis in shared memory, `vstride` between
+// variables. The axis is a runtime value so that both directions run the
+// same instructions.
+template <int NDIM, int REC, int LIM, int RS, class T>
+__device__ __forceinline__ void face_sweep(const T* centre, int stride, int vstride, int ntracer, T gamma, T gfac,
+                                           int axis, T* d, T* d_tr) {
     constexpr int nh = 2 + NDIM;
     constexpr int S = stencil_half<REC>();
     T wl[nh], wr[nh];
@@ -238,7 +241,7 @@ __device__ __forceinline__ void face_sweep(const T* centre, int stride, int vstr
         left[v] = __shfl_up_sync(0xffffffffu, wr[v], 1);
     }
     T f[nh];
-    riemann<RS, AXIS, NDIM>(gamma, left, wl, f);
+    riemann<RS, NDIM>(gamma, gfac, axis, left, wl, f);
 #pragma unroll
     for (int v = 0; v < nh; ++v) {
         const T fn = __shfl_down_sync(0xffffffffu, f[v], 1);
@@ -292,7 +295,8 @@ __global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
     const int warp = threadIdx.x >> 5;
     const int cl = warp * kTile + lane - 1;  // cell of this lane, relative to x0
     T d[nh], d_tr[kMaxVars];
-    face_sweep<0, NDIM, REC, LIM, RS, T>(W + H + cl, 1, WN, p.ntracer, T(p.gamma), d, d_tr);
+    const T gfac = T((p.gamma + 1.0) / (2.0 * p.gamma));
+    face_sweep<NDIM, REC, LIM, RS, T>(W + H + cl, 1, WN, p.ntracer, T(p.gamma), gfac, 0, d, d_tr);
 
     const double dt = stage_dt(p);
     const double dtdx = dt / p.dx;
@@ -331,7 +335,7 @@ __global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
 // blockIdx.z, writing the x+y divergence instead of finishing the stage).
 // ---------------------------------------------------------------------------
 template <int NDIM, int REC, int LIM, int RS, class T>
-__global__ void __launch_bounds__(kThreads) stage2d_kernel(StageParams p) {
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : kMinBlocks2d) stage2d_kernel(StageParams p) {
     if (p.dt_dev && p.blk->done) {
         return;
     }
@@ -340,12 +344,10 @@ __global__ void __launch_bounds__(kThreads) stage2d_kernel(StageParams p) {
     using G = TileGeom<2, REC>;
     constexpr int H = G::H, TX = G::TX, TY = G::TY, WX = G::WX, P = G::P, WY = G::WY, PY = G::PY;
     constexpr int WV = WY * P;   // per-variable stride of W
-    constexpr int XV = TY * TX;  // per-variable stride of dQx
-    constexpr int YV = TY * PY;  // per-variable stride of dQy
+    constexpr int YV = TY * PY;  // per-variable stride of dFy
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* W = reinterpret_cast<T*>(smem_raw);
-    T* DX = W + (size_t)p.nvar * WV;
-    T* DY = DX + (size_t)p.nvar * XV;
+    T* DY = W + (size_t)p.nvar * WV;
     __shared__ double red_d[kWarps];
     __shared__ unsigned red_u[kWarps];
 
@@ -380,82 +382,84 @@ __global__ void __launch_bounds__(kThreads) stage2d_kernel(StageParams p) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const T gamma = T(p.gamma);
+    const T gfac = T((p.gamma + 1.0) / (2.0 * p.gamma));
     const int ntr = p.ntracer;
-
-    // phase 2: x faces, one warp per row
-    for (int r = warp; r < vh; r += kWarps) {
-        const int cx = lane - 1;
-        T d[nh], d_tr[kMaxVars];
-        face_sweep<0, NDIM, REC, LIM, RS, T>(W + (r + H) * P + (cx + H), 1, WV, ntr, gamma, d, d_tr);
-        if (lane >= 1 && lane <= TX) {
-#pragma unroll
-            for (int v = 0; v < nh; ++v) {
-                DX[v * XV + r * TX + cx] = d[v];
-            }
-            for (int t = 0; t < ntr; ++t) {
-                DX[(nh + t) * XV + r * TX + cx] = d_tr[t];
-            }
-        }
-    }
-    // phase 3: y faces, one warp per column
-    for (int c = warp; c < vw; c += kWarps) {
-        const int cy = lane - 1;
-        T d[nh], d_tr[kMaxVars];
-        face_sweep<1, NDIM, REC, LIM, RS, T>(W + (cy + H) * P + (c + H), P, WV, ntr, gamma, d, d_tr);
-        if (lane >= 1 && lane <= TY) {
-#pragma unroll
-            for (int v = 0; v < nh; ++v) {
-                DY[v * YV + cy * PY + c] = d[v];
-            }
-            for (int t = 0; t < ntr; ++t) {
-                DY[(nh + t) * YV + cy * PY + c] = d_tr[t];
-            }
-        }
-    }
-    __syncthreads();
-
-    // phase 4: stage update (2D) or x+y divergence (3D)
     const double dt = stage_dt(p);
     const double dtdx = dt / p.dx;
+    const bool old = combo_reads_old(p.combo);
     double dtmin = __longlong_as_double(0x7ff0000000000000ll);
-    for (int it = threadIdx.x; it < TX * TY; it += kThreads) {
-        const int ty = it / TX;
-        const int tx = it - ty * TX;
-        if (tx >= vw || ty >= vh) {
-            continue;
-        }
-        const int i = p.ng + x0 + tx;
-        const int j = p.ng + y0 + ty;
-        if constexpr (NDIM == 3) {
-            const long long cells = (long long)p.nx * p.ny * p.nz;
-            const long long o = ((long long)(k - p.ng) * p.ny + (j - p.ng)) * p.nx + (i - p.ng);
-            for (int v = 0; v < p.nvar; ++v) {
-                double qu = 0.0;
-                qu += double(DX[v * XV + ty * TX + tx]);
-                qu += double(DY[v * YV + ty * PY + tx]);
-                p.dqxy[v * cells + o] = qu;
-            }
-        } else {
-            double qn[kMaxVars];
+    const int c = lane - 1;  // this lane's cell along the sweep
+
+    // Two passes through one copy of the sweep code. Pass 0: y faces, one warp
+    // per column, divergence into DY. Pass 1: x faces, one warp per row; the
+    // lane of each cell then finishes it: q_update = (0 + dFx) + dFy as in
+    // integrate_flux (source/TimeStepping.cpp:22-27), the stage combination,
+    // the store and the ghost scatter (2D), or the x+y divergence (3D).
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+        const int axis = 1 - pass;
+        const int nlines = axis == 1 ? vw : vh;
+        for (int line = warp; line < nlines; line += kWarps) {
+            const T* centre = axis == 0 ? W + (line + H) * P + (c + H) : W + (c + H) * P + (line + H);
+            T d[nh], d_tr[kMaxVars];
+            face_sweep<NDIM, REC, LIM, RS, T>(centre, axis == 0 ? 1 : P, WV, ntr, gamma, gfac, axis, d, d_tr);
+            const bool mine = lane >= 1 && lane <= kTile;
+            if (axis == 1) {
+                if (mine) {
+                    T* dst = DY + c * PY + line;
 #pragma unroll
-            for (int v = 0; v < kMaxVars; ++v) {
-                qn[v] = 0.0;
-            }
-#pragma unroll
-            for (int v = 0; v < kMaxVars; ++v) {
-                if (v < p.nvar) {
-                    double qu = 0.0;
-                    qu += double(DX[v * XV + ty * TX + tx]);
-                    qu += double(DY[v * YV + ty * PY + tx]);
-                    qu *= dtdx;
-                    const double src = (v < nh) ? 0.0 * dt : 0.0;
-                    const long long id = qidx(p, v, 0, j, i);
-                    const double qo = combo_reads_old(p.combo) ? p.q_old[id] : 0.0;
-                    qn[v] = combine(p.combo, qo, p.q_in[id], qu, src);
+                    for (int v = 0; v < nh; ++v) {
+                        dst[v * YV] = d[v];
+                    }
+                    for (int t = 0; t < ntr; ++t) {
+                        dst[(nh + t) * YV] = d_tr[t];
+                    }
                 }
+                continue;
             }
-            dtmin = smin(write_cell<NDIM>(p, i, j, 0, qn, p.last != 0, &flags), dtmin);
+            if (!mine || c >= vw) {
+                continue;
+            }
+            const T* dfy = DY + line * PY + c;
+            const int i = p.ng + x0 + c;
+            const int j = p.ng + y0 + line;
+            if constexpr (NDIM == 3) {
+                const long long cells = (long long)p.nx * p.ny * p.nz;
+                const long long o = ((long long)(k - p.ng) * p.ny + (j - p.ng)) * p.nx + (i - p.ng);
+#pragma unroll
+                for (int v = 0; v < nh; ++v) {
+                    double qu = 0.0;
+                    qu += double(d[v]);
+                    qu += double(dfy[v * YV]);
+                    p.dqxy[v * cells + o] = qu;
+                }
+            } else {
+                double qn[kMaxVars];
+#pragma unroll
+                for (int v = 0; v < kMaxVars; ++v) {
+                    qn[v] = 0.0;
+                }
+#pragma unroll
+                for (int v = 0; v < nh; ++v) {
+                    double qu = 0.0;
+                    qu += double(d[v]);
+                    qu += double(dfy[v * YV]);
+                    qu *= dtdx;
+                    const long long id = qidx(p, v, 0, j, i);
+                    qn[v] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0 * dt);
+                }
+                for (int t = 0; t < ntr; ++t) {
+                    double qu = 0.0;
+                    qu += double(d_tr[t]);
+                    qu += double(dfy[(nh + t) * YV]);
+                    qu *= dtdx;
+                    const long long id = qidx(p, nh + t, 0, j, i);
+                    qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0);
+                }
+                dtmin = smin(write_cell<NDIM>(p, i, j, 0, qn, p.last != 0, &flags), dtmin);
+            }
         }
+        __syncthreads();
     }
     block_publish(dtmin, flags, NDIM != 3 && p.last != 0, p.blk, red_d, red_u);
 }
@@ -488,6 +492,7 @@ __global__ void __launch_bounds__(kZBlockX* kZBlockY) zsweep3d_kernel(StageParam
     const bool active = xi < p.nx && yi < p.ny;
     const int i = xi + p.ng, j = yi + p.ng;
     const T gamma = T(p.gamma);
+    const T gfac = T((p.gamma + 1.0) / (2.0 * p.gamma));
     const double dt = stage_dt(p);
     const double dtdx = dt / p.dx;
     const long long cells = (long long)p.nx * p.ny * p.nz;
@@ -547,7 +552,7 @@ __global__ void __launch_bounds__(kZBlockX* kZBlockY) zsweep3d_kernel(StageParam
         }
         shift_in(z0 + S);
         recon_window(rl_cur, rr_cur);  // cell z0
-        riemann<RS, 2, NDIM>(gamma, rr_prev, rl_cur, f_prev);  // face z0 - 1/2
+        riemann<RS, NDIM>(gamma, gfac, 2, rr_prev, rl_cur, f_prev);  // face z0 - 1/2
 #pragma unroll
         for (int v = 0; v < nh; ++v) {
             rr_prev[v] = rr_cur[v];
@@ -555,7 +560,7 @@ __global__ void __launch_bounds__(kZBlockX* kZBlockY) zsweep3d_kernel(StageParam
         for (int z = z0; z < z1; ++z) {
             shift_in(z + 1 + S);
             recon_window(rl_cur, rr_cur);  // cell z+1
-            riemann<RS, 2, NDIM>(gamma, rr_prev, rl_cur, f_cur);  // face z + 1/2
+            riemann<RS, NDIM>(gamma, gfac, 2, rr_prev, rl_cur, f_cur);  // face z + 1/2
             const int kk = z + p.ng;
             const long long o = ((long long)z * p.ny + yi) * p.nx + xi;
             double qn[kMaxVars];

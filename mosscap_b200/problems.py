@@ -175,6 +175,66 @@ def sedov_3d(n: int = 512, ng: int = 3, e_blast: float = 1.0, max_cfl: float = 0
     return p
 
 
+def riemann_batch(seed: int = 0, n1d: int = 2048, n2d: int = 2048, riemann_solver: str = "hllc",
+                  min1d: int = 64, max1d: int = 4096, min2d: int = 64, max2d: int = 512,
+                  max_cfl: float = 0.8, steps_time: float = 1e30, ng: int = 3) -> List[Problem]:
+    """Independent Riemann problems of uneven size from one seed.
+
+    1D: a shock tube with cell count log-uniform in [min1d, max1d] on [0,1],
+    left / right states split at x = 0.5. 2D: a four-quadrant problem on
+    [0,1]^2, side log-uniform in [min2d, max2d], one state per quadrant
+    around (0.5, 0.5). Every state draws rho and p log-uniform in
+    [1e-3, 10] and each velocity component uniform in [-2, 2]; gamma 1.4,
+    MUSCL (minmod), ``riemann_solver``, SSPRK2 (``rk2``), zero-gradient
+    boundaries, CFL ``max_cfl`` per problem (its own dt). The 2D CFL is
+    ``max_cfl / 2``: the reference's CFL bound is per direction while its
+    update is unsplit."""
+    rng = np.random.default_rng(seed)
+    out: List[Problem] = []
+
+    def state(nd):
+        rho = float(np.exp(rng.uniform(np.log(1e-3), np.log(10.0))))
+        p = float(np.exp(rng.uniform(np.log(1e-3), np.log(10.0))))
+        v = [float(x) for x in rng.uniform(-2.0, 2.0, size=nd)]
+        return rho, v, p
+
+    for _ in range(n1d):
+        n = int(round(np.exp(rng.uniform(np.log(min1d), np.log(max1d)))))
+        dx = 1.0 / n
+        x = cell_centres(1, n, ng, dx, 0.0)
+        (rl, vl, pl), (rr, vr, pr) = state(1), state(1)
+        left = x < 0.5
+        w = np.empty((3, 1, 1, x.size))
+        w[0, 0, 0] = np.where(left, rl, rr)
+        w[1, 0, 0] = np.where(left, vl[0], vr[0])
+        w[2, 0, 0] = np.where(left, pl, pr)
+        p = Problem(f"tube_{len(out)}", 1, n, ng=ng, dx=dx, bc=("zerograd",) * 6, reconstruction="muscl",
+                    slope_limiter="minmod", riemann_solver=riemann_solver, time_stepper="rk2", gamma=1.4,
+                    max_cfl=max_cfl, max_time=steps_time, output_delta=steps_time)
+        p.Q = prim_to_cons(1, 1.4, w)
+        out.append(p)
+    for _ in range(n2d):
+        n = int(round(np.exp(rng.uniform(np.log(min2d), np.log(max2d)))))
+        dx = 1.0 / n
+        c = cell_centres(2, n, ng, dx, 0.0)
+        X, Y = np.meshgrid(c, c, indexing="xy")
+        quad = (X >= 0.5).astype(int) + 2 * (Y >= 0.5).astype(int)
+        w = np.empty((4, 1, c.size, c.size))
+        for qd in range(4):
+            rho, v, pr = state(2)
+            m = quad == qd
+            w[0, 0][m] = rho
+            w[1, 0][m] = v[0]
+            w[2, 0][m] = v[1]
+            w[3, 0][m] = pr
+        p = Problem(f"quadrant_{len(out)}", 2, n, n, ng=ng, dx=dx, bc=("zerograd",) * 6, reconstruction="muscl",
+                    slope_limiter="minmod", riemann_solver=riemann_solver, time_stepper="rk2", gamma=1.4,
+                    max_cfl=max_cfl / 2.0, max_time=steps_time, output_delta=steps_time)
+        p.Q = prim_to_cons(2, 1.4, w)
+        out.append(p)
+    return out
+
+
 def random_state(num_dim: int, nx: int, ny: int = 1, nz: int = 1, ng: int = 3,
                  num_tracers: int = 0, seed: int = 0, jumps: bool = True,
                  gamma: float = 1.4, vmax: float = 1.0) -> np.ndarray:
