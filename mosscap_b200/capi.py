@@ -63,6 +63,15 @@ class McClock(ctypes.Structure):
     ]
 
 
+class McBatchProblem(ctypes.Structure):
+    _fields_ = [
+        ("grid", McGrid),
+        ("offset", ctypes.c_int64),
+        ("max_cfl", ctypes.c_double),
+        ("clock", McClock),
+    ]
+
+
 USER_BC_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
 
 
@@ -109,6 +118,20 @@ def load() -> ctypes.CDLL:
     lib.mc_profile_stages.restype = i32
     lib.mc_stage_time.argtypes = [vp, i32, P(d), P(i64)]
     lib.mc_stage_time.restype = i32
+    lib.mc_batch_create.argtypes = [P(McBatchProblem), i32, P(McScheme), i64, P(vp)]
+    lib.mc_batch_create.restype = i32
+    lib.mc_batch_destroy.argtypes = [vp]
+    lib.mc_batch_destroy.restype = i32
+    lib.mc_batch_fill_bcs.argtypes = [vp, vp, vp]
+    lib.mc_batch_fill_bcs.restype = i32
+    lib.mc_batch_tune.argtypes = [vp, vp, vp]
+    lib.mc_batch_tune.restype = i32
+    lib.mc_batch_advance.argtypes = [vp, vp, i64, vp]
+    lib.mc_batch_advance.restype = i32
+    lib.mc_batch_clocks.argtypes = [vp, P(McClock), P(i64), P(ctypes.c_uint32), vp]
+    lib.mc_batch_clocks.restype = i32
+    lib.mc_batch_schedule.argtypes = [vp, P(i32), P(i32), P(i32)]
+    lib.mc_batch_schedule.restype = i32
     lib.mc_time_step_noalloc.argtypes = [P(McGrid), P(McScheme), vp, d, vp]
     lib.mc_time_step_noalloc.restype = i32
     lib.mc_launch_count.argtypes = [vp]

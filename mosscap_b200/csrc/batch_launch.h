@@ -1,0 +1,17 @@
+// Host-side declarations of the batched-stage launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "batch_kernels.cuh"
+
+namespace mc {
+
+// Launch one batched stage on `grid` CTAs; with occupancy != NULL, only
+// report the resident CTAs per SM of that kernel instead.
+cudaError_t launch_batch_stage_fp64(const BatchStageParams& bp, int rec, int lim, int rs, int grid, cudaStream_t s,
+                                    int* occupancy);
+cudaError_t launch_batch_stage_fp32(const BatchStageParams& bp, int rec, int lim, int rs, int grid, cudaStream_t s,
+                                    int* occupancy);
+
+} // namespace mc

@@ -261,4 +261,54 @@ __device__ __forceinline__ void block_publish(double v, unsigned flags, bool do_
     }
 }
 
+// Close the step that just finished (unless `first`) and pick the next dt
+// of one problem's clock:
+//   time += dt; an output falls due when time >= prev_output_time + delta
+//   (source/main.cpp:67-71), which sets prev_output_time = time
+//   (source/Output.cpp:272); the loop ends once time >= max_time
+//   (source/main.cpp:54), and, with stop_at_output, also after a step that
+//   made an output due (so that the host can write it);
+//   dt = max_cfl * min, clamped to end exactly on the next output time
+//   (source/Hydro.cpp:231-241).
+__device__ __forceinline__ void advance_clock(DeviceBlock* blk, double* dt_log, bool first, bool stop_at_output) {
+    if (blk->done) {
+        return;
+    }
+    const double m = __longlong_as_double((long long)blk->cfl_min_bits);
+    blk->cfl_min_bits = kInfBits;
+    blk->last_cfl_min = m;
+    if (!first) {
+        blk->time += blk->dt;
+        blk->steps += 1;
+        bool stop = false;
+        if (blk->time >= blk->prev_output_time + blk->output_delta) {
+            blk->prev_output_time = blk->time;
+            stop = stop_at_output;
+        }
+        if (!(blk->time < blk->max_time)) {
+            stop = true;
+        }
+        if (stop) {
+            blk->done = 1;
+            return;
+        }
+    }
+    double dt = m * blk->max_cfl;
+    const double next_write = smin(blk->max_time, blk->prev_output_time + blk->output_delta);
+    if (blk->time + dt >= next_write) {
+        dt = next_write - blk->time;
+        while (blk->time + dt < next_write) {
+            dt = nextafter(dt, 1.7976931348623157e308);
+        }
+    }
+    blk->dt = dt;
+    if (dt_log) {
+        dt_log[blk->steps] = dt;
+    }
+    if (!(dt > 0.0) || !isfinite(dt)) {
+        blk->status |= 0x8u;
+        blk->done = 1;
+    }
+}
+
 } // namespace mc

@@ -59,7 +59,7 @@ struct TileGeom {
 template <int NDIM, int REC>
 __host__ __device__ constexpr int smem_w_per_var() {
     using G = TileGeom<NDIM, REC>;
-    return NDIM == 1 ? (kWarps * kTile + 2 * G::H) : G::WY * G::P;
+    return NDIM == 1 ? kWarps * (kTile + 2 * G::H) : G::WY * G::P;
 }
 template <int NDIM, int REC>
 __host__ __device__ constexpr int smem_dqy_per_var() {
@@ -264,43 +264,37 @@ __device__ __forceinline__ void face_sweep(const T* centre, int stride, int vstr
 }
 
 // ---------------------------------------------------------------------------
-// 1D stage kernel: a CTA owns kWarps segments of kTile cells.
+// 1D: one warp updates one segment of kTile cells, independently of the
+// other warps of its CTA (so one CTA can serve segments of different
+// problems in a batch). W is this warp's shared window of
+// nvar x (kTile + 2H) primitives.
 // ---------------------------------------------------------------------------
+template <int REC>
+__host__ __device__ constexpr int seg1d_window() {
+    return kTile + 2 * halo_of<REC>();
+}
+
 template <int REC, int LIM, int RS, class T>
-__global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
-    if (p.dt_dev && p.blk->done) {
-        return;
-    }
-    maybe_reset_min(p);
+__device__ __forceinline__ void segment1d(const StageParams& p, int x0, T* W, double& dtmin, unsigned& flags) {
     constexpr int NDIM = 1;
     constexpr int nh = 3;
-    using G = TileGeom<1, REC>;
-    constexpr int H = G::H;
-    constexpr int WN = kWarps * kTile + 2 * H;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red_d[kWarps];
-    __shared__ unsigned red_u[kWarps];
-    T* W = reinterpret_cast<T*>(smem_raw);
-
-    const int x0 = blockIdx.x * (kWarps * kTile);  // first interior cell of the CTA
-    unsigned flags = 0;
-    for (int it = threadIdx.x; it < WN; it += kThreads) {
+    constexpr int H = halo_of<REC>();
+    constexpr int WN = seg1d_window<REC>();
+    const int lane = threadIdx.x & 31;
+    for (int it = lane; it < WN; it += 32) {
         const int i = p.ng + x0 - H + it;  // array index
         const bool inb = i >= 0 && i < p.xc;
         flags |= load_prim<NDIM, T>(p, 0, 0, i, inb, W + it, WN);
     }
-    __syncthreads();
-
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int cl = warp * kTile + lane - 1;  // cell of this lane, relative to x0
+    __syncwarp();
+    const int cl = lane - 1;  // cell of this lane, relative to x0
     T d[nh], d_tr[kMaxVars];
     const T gfac = T((p.gamma + 1.0) / (2.0 * p.gamma));
     face_sweep<NDIM, REC, LIM, RS, T>(W + H + cl, 1, WN, p.ntracer, T(p.gamma), gfac, 0, d, d_tr);
+    __syncwarp();  // the window may be reloaded by the caller's next segment
 
     const double dt = stage_dt(p);
     const double dtdx = dt / p.dx;
-    double dtmin = __longlong_as_double(0x7ff0000000000000ll);
     const int cell = x0 + cl;  // interior index
     if (lane >= 1 && lane <= kTile && cell < p.nx) {
         const int i = cell + p.ng;
@@ -325,7 +319,27 @@ __global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
             const long long id = qidx(p, nh + t, 0, 0, i);
             qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0);
         }
-        dtmin = write_cell<NDIM>(p, i, 0, 0, qn, p.last != 0, &flags);
+        dtmin = smin(write_cell<NDIM>(p, i, 0, 0, qn, p.last != 0, &flags), dtmin);
+    }
+}
+
+// 1D stage kernel: warp w of CTA b updates segment b * kWarps + w.
+template <int REC, int LIM, int RS, class T>
+__global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
+    if (p.dt_dev && p.blk->done) {
+        return;
+    }
+    maybe_reset_min(p);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red_d[kWarps];
+    __shared__ unsigned red_u[kWarps];
+    const int warp = threadIdx.x >> 5;
+    T* W = reinterpret_cast<T*>(smem_raw) + (size_t)warp * p.nvar * seg1d_window<REC>();
+    double dtmin = __longlong_as_double(0x7ff0000000000000ll);
+    unsigned flags = 0;
+    const int x0 = (blockIdx.x * kWarps + warp) * kTile;
+    if (x0 < p.nx) {
+        segment1d<REC, LIM, RS, T>(p, x0, W, dtmin, flags);
     }
     block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
 }
@@ -334,31 +348,27 @@ __global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
 // 2D stage kernel, and the x-y pass of 3D (NDIM == 3: one z plane per
 // blockIdx.z, writing the x+y divergence instead of finishing the stage).
 // ---------------------------------------------------------------------------
+// One CTA updates tile (bx, by) of a 2D problem, or of z plane bz in the 3D
+// plane pass. smem holds nvar x (WY x P) primitives and nvar x (TY x PY)
+// y divergences. Contains CTA-wide barriers: every thread of the CTA calls it.
 template <int NDIM, int REC, int LIM, int RS, class T>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : kMinBlocks2d) stage2d_kernel(StageParams p) {
-    if (p.dt_dev && p.blk->done) {
-        return;
-    }
-    maybe_reset_min(p);
+__device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int bz, T* smem, double& dtmin,
+                                       unsigned& flags) {
     constexpr int nh = 2 + NDIM;
     using G = TileGeom<2, REC>;
     constexpr int H = G::H, TX = G::TX, TY = G::TY, WX = G::WX, P = G::P, WY = G::WY, PY = G::PY;
     constexpr int WV = WY * P;   // per-variable stride of W
     constexpr int YV = TY * PY;  // per-variable stride of dFy
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* W = reinterpret_cast<T*>(smem_raw);
+    T* W = smem;
     T* DY = W + (size_t)p.nvar * WV;
-    __shared__ double red_d[kWarps];
-    __shared__ unsigned red_u[kWarps];
 
-    const int x0 = blockIdx.x * TX;
-    const int y0 = blockIdx.y * TY;
-    const int k = NDIM == 3 ? p.ng + blockIdx.z : 0;
+    const int x0 = bx * TX;
+    const int y0 = by * TY;
+    const int k = NDIM == 3 ? p.ng + bz : 0;
     const int vw = min(TX, p.nx - x0);
     const int vh = min(TY, p.ny - y0);
 
     // phase 1: primitives of the tile and its cross-shaped halo
-    unsigned flags = 0;
     constexpr int core = TY * WX;
     constexpr int items = core + 2 * H * TX;
     for (int it = threadIdx.x; it < items; it += kThreads) {
@@ -387,7 +397,6 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : k
     const double dt = stage_dt(p);
     const double dtdx = dt / p.dx;
     const bool old = combo_reads_old(p.combo);
-    double dtmin = __longlong_as_double(0x7ff0000000000000ll);
     const int c = lane - 1;  // this lane's cell along the sweep
 
     // Two passes through one copy of the sweep code. Pass 0: y faces, one warp
@@ -461,6 +470,22 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : k
         }
         __syncthreads();
     }
+}
+
+template <int NDIM, int REC, int LIM, int RS, class T>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : kMinBlocks2d)
+    stage2d_kernel(StageParams p) {
+    if (p.dt_dev && p.blk->done) {
+        return;
+    }
+    maybe_reset_min(p);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red_d[kWarps];
+    __shared__ unsigned red_u[kWarps];
+    double dtmin = __longlong_as_double(0x7ff0000000000000ll);
+    unsigned flags = 0;
+    tile2d<NDIM, REC, LIM, RS, T>(p, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<T*>(smem_raw), dtmin,
+                                  flags);
     block_publish(dtmin, flags, NDIM != 3 && p.last != 0, p.blk, red_d, red_u);
 }
 

@@ -85,52 +85,8 @@ __global__ void clock_init_kernel(DeviceBlock* blk, double time, double max_time
     blk->done = time < max_time ? 0 : 1;
 }
 
-// Close the step that just finished (unless `first`) and pick the next dt:
-//   time += dt; an output falls due when time >= prev_output_time + delta
-//   (source/main.cpp:67-71, which then sets prev_output_time = time,
-//   source/Output.cpp:272); the loop stops after such a step or once
-//   time >= max_time (source/main.cpp:54);
-//   dt = max_cfl * min, clamped to end exactly on the next output time
-//   (source/Hydro.cpp:231-241).
 __global__ void clock_advance_kernel(DeviceBlock* blk, double* dt_log, int first) {
-    if (blk->done) {
-        return;
-    }
-    const double m = __longlong_as_double((long long)blk->cfl_min_bits);
-    blk->cfl_min_bits = kInfBits;
-    blk->last_cfl_min = m;
-    if (!first) {
-        blk->time += blk->dt;
-        blk->steps += 1;
-        bool stop = false;
-        if (blk->time >= blk->prev_output_time + blk->output_delta) {
-            blk->prev_output_time = blk->time;
-            stop = true;
-        }
-        if (!(blk->time < blk->max_time)) {
-            stop = true;
-        }
-        if (stop) {
-            blk->done = 1;
-            return;
-        }
-    }
-    double dt = m * blk->max_cfl;
-    const double next_write = smin(blk->max_time, blk->prev_output_time + blk->output_delta);
-    if (blk->time + dt >= next_write) {
-        dt = next_write - blk->time;
-        while (blk->time + dt < next_write) {
-            dt = nextafter(dt, 1.7976931348623157e308);
-        }
-    }
-    blk->dt = dt;
-    if (dt_log) {
-        dt_log[blk->steps] = dt;
-    }
-    if (!(dt > 0.0) || !isfinite(dt)) {
-        blk->status |= 0x8u;
-        blk->done = 1;
-    }
+    advance_clock(blk, dt_log, first != 0, true);
 }
 
 } // namespace

@@ -184,3 +184,114 @@ class HydroSim:
 
     def get_Q(self) -> np.ndarray:
         return self.Q.detach().cpu().numpy()
+
+
+def grid_of(p: Problem) -> capi.McGrid:
+    """The mc_grid of a Problem."""
+    g = capi.McGrid()
+    shape = p.shape
+    g.num_dim = p.num_dim
+    g.zc, g.yc, g.xc = shape[1], shape[2], shape[3]
+    g.ng = p.ng
+    g.num_tracers = p.num_tracers
+    g.dx = p.dx
+    for a in range(3):
+        g.loc[a] = p.loc[a]
+    for f in range(6):
+        g.bc[f] = capi.BOUNDARY[p.bc[f]]
+    return g
+
+
+class BatchSim:
+    """Many independent 1D / 2D problems advanced together (mc_batch_*).
+
+    The problems' states live in one float64 pool on the GPU, each problem's
+    ``[var][zc][yc][xc]`` block at its own offset. Every problem runs its own
+    main loop with its own dt; ``advance(k)`` replays the captured step graph
+    k times."""
+
+    def __init__(self, problems: Sequence[Problem], precision: str = "fp64",
+                 device: Optional[torch.device] = None):
+        self.lib = capi.load()
+        self.device = torch.device(device or "cuda")
+        self.problems = list(problems)
+        p0 = self.problems[0]
+        offs, total = [], 0
+        for p in self.problems:
+            offs.append(total)
+            total += int(np.prod(p.shape))
+            total = (total + 31) // 32 * 32  # 256-byte aligned blocks
+        self.offsets = offs
+        pool = np.zeros(total, dtype=np.float64)
+        for p, o in zip(self.problems, offs):
+            pool[o:o + int(np.prod(p.shape))] = np.ascontiguousarray(p.Q, dtype=np.float64).ravel()
+        self.pool = torch.from_numpy(pool).to(self.device)
+        arr = (capi.McBatchProblem * len(self.problems))()
+        for k, (p, o) in enumerate(zip(self.problems, offs)):
+            arr[k].grid = grid_of(p)
+            arr[k].offset = o
+            arr[k].max_cfl = p.max_cfl
+            arr[k].clock.time = 0.0
+            arr[k].clock.max_time = p.max_time
+            arr[k].clock.prev_output_time = 0.0
+            arr[k].clock.output_delta = p.output_delta
+        s = capi.McScheme()
+        s.reconstruction = capi.RECON[p0.reconstruction]
+        s.slope_limiter = capi.LIMITER[p0.slope_limiter]
+        s.riemann_solver = capi.RIEMANN[p0.riemann_solver]
+        s.time_stepper = capi.STEPPER[p0.time_stepper]
+        s.precision = capi.PRECISION[precision]
+        s.gamma = p0.gamma
+        s.max_cfl = p0.max_cfl
+        self._problems_c, self._scheme = arr, s
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            capi.check(self.lib.mc_batch_create(arr, len(self.problems), ctypes.byref(s), total, ctypes.byref(h)),
+                       "mc_batch_create")
+        self.ctx = h
+
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self.lib.mc_batch_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def _pool(self):
+        return ctypes.c_void_p(self.pool.data_ptr())
+
+    def fill_bcs(self) -> None:
+        capi.check(self.lib.mc_batch_fill_bcs(self.ctx, self._pool(), self._stream()), "mc_batch_fill_bcs")
+
+    def tune(self):
+        capi.check(self.lib.mc_batch_tune(self.ctx, self._pool(), self._stream()), "mc_batch_tune")
+        return self.schedule()
+
+    def schedule(self):
+        g, d, s = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        capi.check(self.lib.mc_batch_schedule(self.ctx, ctypes.byref(g), ctypes.byref(d), ctypes.byref(s)),
+                   "mc_batch_schedule")
+        return {"grid": g.value, "dynamic": bool(d.value), "segments_per_task": s.value}
+
+    def advance(self, steps: int) -> None:
+        capi.check(self.lib.mc_batch_advance(self.ctx, self._pool(), int(steps), self._stream()), "mc_batch_advance")
+
+    def clocks(self):
+        n = len(self.problems)
+        clk = (capi.McClock * n)()
+        steps = (ctypes.c_int64 * n)()
+        status = (ctypes.c_uint32 * n)()
+        capi.check(self.lib.mc_batch_clocks(self.ctx, clk, steps, status, self._stream()), "mc_batch_clocks")
+        return (np.array([c.time for c in clk]), np.array(list(steps)), np.array(list(status)))
+
+    def get_Q(self, k: int) -> np.ndarray:
+        p = self.problems[k]
+        n = int(np.prod(p.shape))
+        return self.pool[self.offsets[k]:self.offsets[k] + n].view(p.shape).cpu().numpy()
