@@ -47,9 +47,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_CELLS_SIDE, help="cells per side (default 2048)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--workload", default="kh2d", choices=["kh2d", "sedov3d", "batch"],
+    ap.add_argument("--workload", default="kh2d", choices=["kh2d", "sedov3d", "batch", "adjoint"],
                     help="kh2d: the headline line; sedov3d and batch print their own lines")
     ap.add_argument("--solver", default="hllc", choices=["hllc", "rusanov"], help="batch workload solver")
+    ap.add_argument("--fd-directions", type=int, default=64, help="adjoint workload: finite-difference checks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -179,7 +180,8 @@ def run_reference(args):
     if rank != 0:
         return
     n = args.n
-    value, done, secs, kind, cores = cpu_run(n, args.steps, args.warmup)
+    # a bounded sample: at most K steps and at most ~2 minutes of CPU work
+    value, done, secs, kind, cores = cpu_run(n, args.steps, min(args.warmup, 2), budget_s=120.0)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * secs / done, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -375,8 +377,75 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args):
+    """Adjoint of KH 512^2 (WENO5-Z + HLLC, SSPRK3, FP64): forward run of K
+    steps with checkpoints every 20, then the reverse sweep; reports the
+    adjoint : forward cost ratio (CUDA events on the launching stream)."""
+    import torch
+    from mosscap_b200 import problems as P
+    from mosscap_b200.adjoint import EulerSteps, kh_initial_state, kh_vy
+    n = args.n if args.n != N_CELLS_SIDE else 512
+    steps = args.steps
+    p = P.kelvin_helmholtz_2d(n, seed=0)
+    pt = P.kelvin_helmholtz_2d(n, seed=1)
+    dev = torch.device("cuda")
+    with torch.no_grad():
+        gt = torch.tensor(pt.gamma, dtype=torch.float64, device=dev)
+        vyt = torch.tensor(kh_vy(pt), device=dev)
+        rho_t = EulerSteps.apply(kh_initial_state(vyt, gt, pt), gt, pt, steps, 1 << 30)[0].clone()
+    vy = torch.tensor(kh_vy(p), device=dev, requires_grad=True)
+    g = torch.tensor(p.gamma, dtype=torch.float64, device=dev, requires_grad=True)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    e[0].record()
+    q = EulerSteps.apply(kh_initial_state(vy, g, p), g, p, steps, 20)
+    J = 0.5 * ((q[0] - rho_t) ** 2).sum()
+    e[1].record()
+    J.backward()
+    e[2].record()
+    torch.cuda.synchronize()
+    fwd, bwd = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    # central finite differences along random unit directions of (vy, gamma):
+    # the vy part with a step below the gap between near-tied CFL arg-min
+    # candidates, the gamma part with a step clear of roundoff
+    gvy, gg = vy.grad.detach(), g.grad.item()
+    rng = np.random.default_rng(2)
+
+    def final_rho(vy_, g_):
+        with torch.no_grad():
+            gt_ = torch.tensor(g_, dtype=torch.float64, device=dev)
+            return EulerSteps.apply(kh_initial_state(vy_, gt_, p), gt_, p, steps, 1 << 30)[0]
+
+    def cdiff(dvy, dg, eps):
+        rp = final_rho(vy.detach() + eps * dvy, p.gamma + eps * dg)
+        rm = final_rho(vy.detach() - eps * dvy, p.gamma - eps * dg)
+        return float((0.5 * (rp - rm) * (rp + rm - 2.0 * rho_t)).sum()) / (2 * eps)
+
+    rels = []
+    for _ in range(args.fd_directions):
+        dvy = torch.tensor(rng.standard_normal((n, n)), device=dev)
+        dvy = dvy / dvy.norm()
+        dg = float(rng.standard_normal()) * 1e-2
+        fd = cdiff(dvy, 0.0, 1e-7) + cdiff(0.0 * dvy, dg, 1e-6)
+        ad = float((gvy * dvy).sum()) + gg * dg
+        rels.append(abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
+    line = {"metric": "adjoint:forward cost", "value": bwd / fwd, "unit": "ratio", "n_gpus": 1, "steps": steps,
+            "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"kh_2d_{n}x{n}_weno5z_hllc_ssprk3_adjoint_ckpt20", "loss": "1/2 |rho - rho_target|^2",
+                       "gradient": "initial vy field and gamma"},
+            "forward_ms": fwd, "backward_ms": bwd,
+            "forward_zone_updates_per_s": n * n * steps / (fwd / 1e3),
+            "loss": J.item(), "dgamma": g.grad.item(), "grad_vy_norm": vy.grad.norm().item(),
+            "fd_check": {"directions": len(rels), "max_rel_err": max(rels) if rels else None,
+                         "median_rel_err": float(np.median(rels)) if rels else None}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.impl != "reference" and args.workload == "adjoint":
+        run_adjoint(args)
+        return
     if args.impl != "reference" and args.workload == "sedov3d":
         run_sedov(args)
         return

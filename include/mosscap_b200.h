@@ -234,6 +234,31 @@ mc_status mc_batch_clocks(mc_batch* batch, mc_clock* clocks, int64_t* steps, uin
 /* The schedule in use: grid size in CTAs, 1 if dynamic, 1D segments per warp task. */
 mc_status mc_batch_schedule(const mc_batch* batch, int32_t* grid, int32_t* dynamic, int32_t* segs_per_task);
 
+/* ---- Discrete adjoint --------------------------------------------------------
+ *
+ * Reverse-mode derivative of n steps of the 2D scheme (WENO5-Z + HLLC +
+ * SSPRK3, FP64, periodic faces): the exact vector-Jacobian product of the
+ * discrete map the forward kernels compute, including each step's dt (the
+ * CFL minimum, through its arg-min cell) and gamma. Reconstruction weights,
+ * HLLC wave-speed choices and min / max / |x| are differentiated along the
+ * branch the forward computation takes. The forward run stores the state
+ * every checkpoint_every steps; the reverse sweep recomputes each segment
+ * from its checkpoint. No counterpart in the reference. */
+typedef struct mc_adjoint mc_adjoint;
+
+mc_status mc_adjoint_create(const mc_grid* grid, const mc_scheme* scheme, int32_t checkpoint_every,
+                            mc_adjoint** out);
+mc_status mc_adjoint_destroy(mc_adjoint* adj);
+/* Advance Q (ghosts filled) by exactly n_steps steps in place, each with
+ * dt = compute_dt under *clock (which must not reach max_time within the run),
+ * recording dt, the CFL minimum and the checkpoints. */
+mc_status mc_adjoint_forward(mc_adjoint* adj, double* Q, const mc_clock* clock, int64_t n_steps, void* stream);
+/* lambda: on entry dJ/dQ of the final state, on exit dJ/dQ of the initial
+ * state (interior cells; the layout of Q). *dgamma (if not NULL) receives
+ * dJ/dgamma through the steps (the initial state held fixed). Waits for the
+ * stream when dgamma is not NULL. */
+mc_status mc_adjoint_backward(mc_adjoint* adj, double* lambda, double* dgamma, void* stream);
+
 /* One SSPRK step in place on Q, like mc_time_step, without a context and
  * without allocating any device memory. No counterpart in the reference.
  *

@@ -38,10 +38,14 @@ def nvcc() -> str:
 
 def _flags_for(src: str) -> list:
     name = os.path.basename(src)
-    exact = "_fp32" not in name
-    # the FP32 compute form is not bit-exact by design: approximate FP32
-    # division / square root and contraction (FP64 division stays IEEE)
-    return ["-fmad=false"] if exact else ["--use_fast_math"]
+    if "_fp32" in name:
+        # the FP32 compute form is not bit-exact by design: approximate FP32
+        # division / square root and contraction (FP64 division stays IEEE)
+        return ["--use_fast_math"]
+    if "_fma" in name:
+        # arithmetic that need not be bit-exact (the adjoint's reverse sweep)
+        return ["-fmad=true"]
+    return ["-fmad=false"]
 
 
 def _headers_mtime() -> float:

@@ -29,4 +29,12 @@ cudaError_t launch_clock_advance(DeviceBlock* blk, double* dt_log, int first, cu
 // Record the message mc_last_error returns on this thread (capi.cu).
 void set_last_error(const char* msg);
 
+// Discrete adjoint, bit-exact parts (adjoint_exact.cu): the recording clock
+// of the forward run (dt, CFL minimum, clamp flag of step `step`) and the
+// search for the interior cell whose CFL bound equals *m_rec (into *idx).
+cudaError_t launch_record_clock(DeviceBlock* blk, int first, double* dts, double* mins, int* clamped,
+                                long long step, cudaStream_t s);
+cudaError_t launch_cfl_argmin(const double* q, int nx, int ny, int ng, int xc, int yc, double gamma, double dx,
+                              const double* m_rec, int* idx, cudaStream_t s);
+
 } // namespace mc

@@ -1,0 +1,164 @@
+"""Slab decomposition of one 2D problem over ranks (one GPU per rank).
+
+The global grid is split along y into equal slabs, one per rank. Each rank
+advances its slab with the fused kernels; the y faces between slabs are
+MC_BC_USERFN faces whose ghost rows are filled by the boundary hook of the C
+ABI (``mc_set_user_bc``, the counterpart of ``Simulation::user_bc``,
+source/Simulation.hpp:55), which the library calls after every stage and
+after ``mc_fill_bcs``: the hook sends this rank's first / last ``ng``
+interior rows to the neighbours below / above and receives their rows into
+its ghost rows (``torch.distributed`` point-to-point, NCCL between GPUs). The
+step's dt is the global CFL minimum (an all-reduce MIN of the per-rank
+minima, exact because a minimum does not depend on order), clamped to the
+output times as ``compute_dt`` does (source/Hydro.cpp:231-241). A slab run
+is therefore bit-identical to the single-domain run.
+
+The outer y faces keep the global problem's kinds; periodic outer faces are
+exchanged between the last and the first rank.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import replace
+from typing import Optional
+
+import numpy as np
+import torch
+import torch.distributed as dist
+
+from . import capi
+from .hydro import HydroSim
+from .problems import Problem
+
+
+class _CudaArray:
+    """A raw device pointer exposed through __cuda_array_interface__."""
+
+    def __init__(self, ptr: int, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8", "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+def exchange_rows(q: torch.Tensor, ng: int, ny: int, rank: int, world: int, periodic: bool,
+                  group=None) -> None:
+    """Fill the y ghost rows of a slab from its neighbours.
+
+    q: [nvar, 1, ny + 2 ng, xc] (this rank's slab with ghosts). Rows
+    [ng, 2 ng) go to the rank below (its top ghosts), rows [ny, ny + ng) to
+    the rank above (its bottom ghosts). Ranks 0 and world-1 exchange with each
+    other only if the outer faces are periodic; otherwise their outer ghost
+    rows are left to the kernels' own boundary handling."""
+    lo_send = q[:, 0, ng:2 * ng, :].contiguous()
+    hi_send = q[:, 0, ny:ny + ng, :].contiguous()
+    below = rank - 1 if rank > 0 else (world - 1 if periodic else None)
+    above = rank + 1 if rank < world - 1 else (0 if periodic else None)
+    if world == 1:
+        if periodic:
+            q[:, 0, 0:ng, :] = hi_send
+            q[:, 0, ny + ng:ny + 2 * ng, :] = lo_send
+        return
+    lo_recv = torch.empty_like(lo_send)
+    hi_recv = torch.empty_like(hi_send)
+    # Messages travelling down (a slab's first rows to the rank below) come
+    # first, then messages travelling up. With two ranks "below" and "above"
+    # are the same peer, and point-to-point messages between one pair match in
+    # issue order (NCCL has no tags), so both sides must issue the down
+    # exchange before the up exchange.
+    down, up = 1, 2
+    ops = []
+    if below is not None:
+        ops.append(dist.P2POp(dist.isend, lo_send, below, group, tag=down))
+    if above is not None:
+        ops.append(dist.P2POp(dist.irecv, hi_recv, above, group, tag=down))
+    if above is not None:
+        ops.append(dist.P2POp(dist.isend, hi_send, above, group, tag=up))
+    if below is not None:
+        ops.append(dist.P2POp(dist.irecv, lo_recv, below, group, tag=up))
+    if ops:
+        for r in dist.batch_isend_irecv(ops):
+            r.wait()
+    if below is not None:
+        q[:, 0, 0:ng, :] = lo_recv
+    if above is not None:
+        q[:, 0, ny + ng:ny + 2 * ng, :] = hi_recv
+
+
+def clamp_to_output(dt: float, time: float, max_time: float, prev_output_time: float, delta: float) -> float:
+    """The output-time clamp of compute_dt (source/Hydro.cpp:231-241)."""
+    cand = prev_output_time + delta
+    next_write = cand if cand < max_time else max_time
+    if time + dt >= next_write:
+        dt = next_write - time
+        while time + dt < next_write:
+            dt = math.nextafter(dt, math.inf)
+    return dt
+
+
+class SlabSim:
+    """This rank's slab of a 2D problem split along y over `world` ranks."""
+
+    def __init__(self, problem: Problem, rank: int = 0, world: int = 1, precision: str = "fp64",
+                 device: Optional[torch.device] = None, group=None):
+        p = problem
+        if p.num_dim != 2 or p.ny % world != 0:
+            raise ValueError("a 2D problem whose row count divides by the number of ranks")
+        self.rank, self.world, self.group = rank, world, group
+        self.ng = p.ng
+        self.ny = p.ny // world
+        self.periodic_y = p.bc[2] == "periodic"
+        bc = list(p.bc)
+        if rank > 0 or self.periodic_y:
+            bc[2] = "userfn"
+        if rank < world - 1 or self.periodic_y:
+            bc[3] = "userfn"
+        ng = p.ng
+        rows = slice(rank * self.ny, rank * self.ny + self.ny + 2 * ng)
+        local = replace(p, ny=self.ny, bc=tuple(bc), loc=(p.loc[0], p.loc[1] + rank * self.ny * p.dx, p.loc[2]),
+                        Q=np.ascontiguousarray(p.Q[:, :, rows, :]))
+        self.problem = local
+        self.sim = HydroSim(local, precision=precision, device=device)
+        self._hook = capi.USER_BC_FN(self._fill_rows)
+        capi.check(self.sim.lib.mc_set_user_bc(self.sim.ctx, self._hook, None), "mc_set_user_bc")
+        self._fused_min_valid = False
+
+    def _fill_rows(self, user, qptr, stream):
+        shape = tuple(self.sim.Q.shape)
+        q = torch.as_tensor(_CudaArray(qptr, shape), device=self.sim.device)
+        exchange_rows(q, self.ng, self.ny, self.rank, self.world, self.periodic_y, self.group)
+
+    @property
+    def time(self) -> float:
+        return self.sim.time
+
+    def fill_bcs(self) -> None:
+        self.sim.fill_bcs()
+        self._fused_min_valid = False
+
+    def compute_dt(self) -> float:
+        """Global dt. After a step the local minimum is the one the step's
+        last stage reduced (interior and x ghosts; the y ghost rows hold
+        neighbours' rows, which the neighbours count), so no extra pass."""
+        if self._fused_min_valid:
+            local = self.sim.last_cfl_min() * self.sim.problem.max_cfl
+        else:
+            local = self.sim.compute_dt(clamp=False)
+        if self.world > 1:
+            t = torch.tensor([local], dtype=torch.float64, device=self.sim.device)
+            dist.all_reduce(t, op=dist.ReduceOp.MIN, group=self.group)
+            local = float(t.item())
+        s = self.sim
+        return clamp_to_output(local, s.time, s.max_time, s.prev_output_time, s.output_delta)
+
+    def step(self) -> float:
+        dt = self.compute_dt()
+        self.sim.time_step(dt)
+        self._fused_min_valid = True
+        s = self.sim
+        if s.time >= s.prev_output_time + s.output_delta:
+            s.prev_output_time = s.time
+        return dt
+
+    def interior(self) -> np.ndarray:
+        ng = self.ng
+        return self.sim.get_Q()[:, :, ng:-ng, ng:-ng]

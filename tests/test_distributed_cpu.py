@@ -1,0 +1,76 @@
+"""Multi-rank host logic of the slab decomposition on CPU: two (and three)
+gloo ranks exchange ghost rows of their slabs; every ghost row must equal the
+neighbouring slab's interior row of the global array (periodic or not)."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, periodic, errors):
+    from mosscap_b200.distributed import exchange_rows
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        ng, ny, nx, nvar = 3, 5, 7, 4
+        rng = np.random.default_rng(0)
+        glob = rng.standard_normal((nvar, 1, world * ny, nx + 2 * ng))
+        # global rows with periodic ghost rows
+        pad = np.concatenate([glob[:, :, -ng:], glob, glob[:, :, :ng]], axis=2)
+        mine = pad[:, :, rank * ny: rank * ny + ny + 2 * ng].copy()
+        q = torch.from_numpy(mine.copy())
+        q[:, 0, :ng] = -1.0
+        q[:, 0, ny + ng:] = -1.0
+        exchange_rows(q, ng, ny, rank, world, periodic)
+        got = q.numpy()
+        exp = mine.copy()
+        if not periodic and rank == 0:
+            exp[:, 0, :ng] = -1.0
+        if not periodic and rank == world - 1:
+            exp[:, 0, ny + ng:] = -1.0
+        if not np.array_equal(got, exp):
+            errors.put(f"rank {rank}: ghost rows differ")
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("periodic", [True, False])
+def test_exchange_rows_gloo(world, periodic):
+    ctx = mp.get_context("spawn")
+    errors = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, periodic, errors)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert errors.empty(), errors.get()
+
+
+def test_clamp_to_output_matches_reference_rule():
+    from mosscap_b200.distributed import clamp_to_output
+    # no clamp
+    assert clamp_to_output(0.01, 0.0, 1.0, 0.0, 0.1) == 0.01
+    # clamped to the next output time, time + dt lands exactly on it
+    t = 0.0949999
+    dt = clamp_to_output(0.01, t, 1.0, 0.0, 0.1)
+    # dt starts at next_write - time and only moves up until time + dt lands
+    assert t + dt >= 0.1 and dt >= 0.1 - t and dt - (0.1 - t) < 1e-17
+    # clamped to max_time
+    dt = clamp_to_output(0.5, 0.9, 1.0, 0.0, 5.0)
+    assert 0.9 + dt >= 1.0

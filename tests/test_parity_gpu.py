@@ -181,3 +181,18 @@ def test_fp32_form_error_bounds(gpu_lib, oracle_port):
     rel_l1 = np.abs(rho - rho_ref).sum() / np.abs(rho_ref).sum()
     assert rel_l1 < 1e-6, rel_l1
     assert sim.status() == 0
+
+
+def test_slab_decomposition_single_rank(gpu_lib, oracle_port):
+    """The slab path (y faces filled by the boundary hook, dt from the
+    step's fused CFL minimum) on one rank with a self-periodic exchange is
+    bit-identical to the reference run of the same periodic problem."""
+    from mosscap_b200.distributed import SlabSim
+    p = P.kelvin_helmholtz_2d(96, seed=5)
+    o = _oracle(oracle_port, p)
+    ref_dts = o.run(8)
+    s = SlabSim(p, rank=0, world=1)
+    s.fill_bcs()
+    dts = [s.step() for _ in range(8)]
+    _assert_same(np.array(dts), ref_dts, "dt")
+    _assert_same(s.sim.get_Q(), o.get_Q(), "state")
