@@ -380,10 +380,14 @@ def run_batch(args):
 def run_adjoint(args):
     """Adjoint of KH 512^2 (WENO5-Z + HLLC, SSPRK3, FP64): forward run of K
     steps with checkpoints every 20, then the reverse sweep; reports the
-    adjoint : forward cost ratio (CUDA events on the launching stream)."""
+    adjoint : forward cost ratio (CUDA events on the launching stream, mean of
+    3 repetitions after warm-up) and a finite-difference check of the
+    gradient along --fd-directions random directions."""
     import torch
     from mosscap_b200 import problems as P
-    from mosscap_b200.adjoint import EulerSteps, kh_initial_state, kh_vy
+    import ctypes
+    from mosscap_b200 import capi
+    from mosscap_b200.adjoint import EulerSteps, _load_adjoint_symbols, _Runner, kh_initial_state, kh_vy, pad_periodic
     n = args.n if args.n != N_CELLS_SIDE else 512
     steps = args.steps
     p = P.kelvin_helmholtz_2d(n, seed=0)
@@ -393,18 +397,48 @@ def run_adjoint(args):
         gt = torch.tensor(pt.gamma, dtype=torch.float64, device=dev)
         vyt = torch.tensor(kh_vy(pt), device=dev)
         rho_t = EulerSteps.apply(kh_initial_state(vyt, gt, pt), gt, pt, steps, 1 << 30)[0].clone()
+    # gradient through the autograd wrapper (the user-facing call)
     vy = torch.tensor(kh_vy(p), device=dev, requires_grad=True)
     g = torch.tensor(p.gamma, dtype=torch.float64, device=dev, requires_grad=True)
-    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    torch.cuda.synchronize()
-    e[0].record()
     q = EulerSteps.apply(kh_initial_state(vy, g, p), g, p, steps, 20)
     J = 0.5 * ((q[0] - rho_t) ** 2).sum()
-    e[1].record()
     J.backward()
-    e[2].record()
+    # cost: the C ABI calls on one mc_adjoint whose buffers a warm-up pass
+    # allocated; forward = mc_adjoint_forward (K steps, checkpoints every 20),
+    # adjoint = mc_adjoint_backward (segment recompute + reverse sweep)
+    _load_adjoint_symbols()
+    runner = _Runner(p, p.gamma, 20)
+    ng = p.ng
+    with torch.no_grad():
+        q0 = pad_periodic(kh_initial_state(vy.detach(), g.detach(), p), ng)
+    stream = runner.stream()
+
+    def one(rec=None):
+        qq = q0.clone()
+        if rec:
+            rec[0].record()
+        runner.forward(qq, steps)
+        if rec:
+            rec[1].record()
+        lam = torch.zeros_like(qq)
+        lam[0, 0, ng:-ng, ng:-ng] = qq[0, 0, ng:-ng, ng:-ng] - rho_t
+        if rec:
+            rec[2].record()
+        capi.check(runner.lib.mc_adjoint_backward(runner.h, ctypes.c_void_p(lam.data_ptr()), None, stream),
+                   "mc_adjoint_backward")
+        if rec:
+            rec[3].record()
+
+    for _ in range(max(args.warmup, 3)):
+        one()
+    reps = 3
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(reps)]
     torch.cuda.synchronize()
-    fwd, bwd = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    for r in range(reps):
+        one(ev[r])
+    torch.cuda.synchronize()
+    fwd = sum(x[0].elapsed_time(x[1]) for x in ev) / reps
+    bwd = sum(x[2].elapsed_time(x[3]) for x in ev) / reps
     # central finite differences along random unit directions of (vy, gamma):
     # the vy part with a step below the gap between near-tied CFL arg-min
     # candidates, the gamma part with a step clear of roundoff
@@ -421,7 +455,7 @@ def run_adjoint(args):
         rm = final_rho(vy.detach() - eps * dvy, p.gamma - eps * dg)
         return float((0.5 * (rp - rm) * (rp + rm - 2.0 * rho_t)).sum()) / (2 * eps)
 
-    rels = []
+    rels, fds, ads = [], [], []
     for _ in range(args.fd_directions):
         dvy = torch.tensor(rng.standard_normal((n, n)), device=dev)
         dvy = dvy / dvy.norm()
@@ -429,6 +463,15 @@ def run_adjoint(args):
         fd = cdiff(dvy, 0.0, 1e-7) + cdiff(0.0 * dvy, dg, 1e-6)
         ad = float((gvy * dvy).sum()) + gg * dg
         rels.append(abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
+        fds.append(fd)
+        ads.append(ad)
+    fds, ads = np.array(fds), np.array(ads)
+    fd_check = {"directions": len(rels), "eps": {"vy": 1e-7, "gamma": 1e-6}, "direction": "unit vy field, gamma 1e-2 N(0,1)"}
+    if rels:
+        fd_check.update({"max_rel_err": max(rels), "median_rel_err": float(np.median(rels)),
+                         "n_within_1e-5": int(sum(r <= 1e-5 for r in rels)),
+                         "aggregate_rel_err": float(np.linalg.norm(fds - ads) / np.linalg.norm(ads)),
+                         "max_abs_err": float(np.abs(fds - ads).max())})
     line = {"metric": "adjoint:forward cost", "value": bwd / fwd, "unit": "ratio", "n_gpus": 1, "steps": steps,
             "higher_is_better": False, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"kh_2d_{n}x{n}_weno5z_hllc_ssprk3_adjoint_ckpt20", "loss": "1/2 |rho - rho_target|^2",
@@ -436,8 +479,7 @@ def run_adjoint(args):
             "forward_ms": fwd, "backward_ms": bwd,
             "forward_zone_updates_per_s": n * n * steps / (fwd / 1e3),
             "loss": J.item(), "dgamma": g.grad.item(), "grad_vy_norm": vy.grad.norm().item(),
-            "fd_check": {"directions": len(rels), "max_rel_err": max(rels) if rels else None,
-                         "median_rel_err": float(np.median(rels)) if rels else None}}
+            "fd_check": fd_check}
     print(json.dumps(line), flush=True)
 
 

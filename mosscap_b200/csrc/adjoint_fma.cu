@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
     const int x0 = blockIdx.x * kAT, y0 = blockIdx.y * kAT;
     const int vw = min(kAT, p.nx - x0), vh = min(kAT, p.ny - y0);
     const double gamma = p.gamma;
+    const mc::GasK K = mc::gas_constants(gamma);
 
     // primitives with a periodic cross-shaped halo of kAH cells
     {
@@ -127,7 +128,7 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
             for (int v = 0; v < 4; ++v) {
                 q[v] = p.q[pidx(p, v, j, i)];
             }
-            mc::prim_from_cons<2>(gamma, q, w);
+            mc::prim_from_cons_rev2(K.gm1, q, w);
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 W[(v * kAW + ty + kAH) * kAP + tx + kAH] = w[v];
@@ -180,7 +181,7 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
                 for (int o = 0; o < 5; ++o) {
                     st[o] = wat(v, o - 2);
                 }
-                mc::reconstruct<mc::kWeno5z, mc::kMonotonizedCentral>(st, rl[v], rr[v]);
+                mc::weno5z_faces(st, rl[v], rr[v]);
             }
             double left[4], mu_r[4], mu_l[4], fb[4];
 #pragma unroll
@@ -192,46 +193,37 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
                 fb[v] = lane >= 1 ? s * (mu_r[v] - mu_l[v]) : 0.0;
             }
             double f[4], wlb[4], wrb[4], gface = 0.0;
-            mc::hllc_vjp2(gamma, axis, left, rl, fb, f, wlb, wrb, &gface);
+            mc::hllc_vjp2(K, axis, left, rl, fb, f, wlb, wrb, &gface);
             // faces 0 .. extent-1 of this line belong to this tile
             const bool own_face = r >= 0 && r < (axis == 0 ? vw : vh);
             if (own_face) {
                 gam += gface;
             }
-            // cotangents of this cell's face values: RL from its own (left)
-            // face, RR from the next face (lane + 1)
-            double rlb[4], rrb[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                rlb[v] = lane >= 1 ? wrb[v] : 0.0;
-                const double nx_l = __shfl_down_sync(0xffffffffu, wlb[v], 1);
-                rrb[v] = lane <= 30 ? nx_l : 0.0;
-            }
-            // divergence of the flux for the dt sensitivity
+            // Per variable: the cotangents of this cell's face values (RL from
+            // its own, left face; RR from the next face, lane + 1), the WENO
+            // VJP onto the stencil, and the gather of the stencil
+            // contributions of cells c-2 .. c+2 into cell c.
             const int c = r;  // tile cell of this lane
             const bool own_cell = c >= 0 && c < (axis == 0 ? vw : vh);
-            double sb_all[4][5];
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
+                const double rlb = lane >= 1 ? wrb[v] : 0.0;
+                const double nx_l = __shfl_down_sync(0xffffffffu, wlb[v], 1);
+                const double rrb = lane <= 30 ? nx_l : 0.0;
+                // divergence of the flux, for the dt sensitivity
                 const double fn = __shfl_down_sync(0xffffffffu, f[v], 1);
                 if (own_cell) {
                     gdt += mu_r[v] * (f[v] - fn);
                 }
-                double st[5];
+                double st[5], sb[5];
 #pragma unroll
                 for (int o = 0; o < 5; ++o) {
                     st[o] = wat(v, o - 2);
-                    sb_all[v][o] = 0.0;
+                    sb[o] = 0.0;
                 }
-                mc::weno5z_vjp(st, rlb[v], rrb[v], sb_all[v]);
-            }
-            // gather the stencil contributions of cells c-2 .. c+2 into cell c
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const double g = __shfl_down_sync(0xffffffffu, sb_all[v][0], 2) +
-                                 __shfl_down_sync(0xffffffffu, sb_all[v][1], 1) + sb_all[v][2] +
-                                 __shfl_up_sync(0xffffffffu, sb_all[v][3], 1) +
-                                 __shfl_up_sync(0xffffffffu, sb_all[v][4], 2);
+                mc::weno5z_vjp(st, rlb, rrb, sb);
+                const double g = __shfl_down_sync(0xffffffffu, sb[0], 2) + __shfl_down_sync(0xffffffffu, sb[1], 1) +
+                                 sb[2] + __shfl_up_sync(0xffffffffu, sb[3], 1) + __shfl_up_sync(0xffffffffu, sb[4], 2);
                 if (own_cell) {
                     double* dst = axis == 0 ? &WB[(v * kAT + line) * kBP + c] : &WB[(v * kAT + c) * kBP + line];
                     *dst += g;
