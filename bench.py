@@ -7,10 +7,14 @@ initial conditions. One bench step = one full SSPRK3 step of the grid
 (mc_advance: dt, the clock and the output clamp never leave the GPU).
 
 Prints one JSON line (rank 0). Metric: zone-updates/s = interior cells x
-steps / time. With --gpus N (one process per GPU under torchrun) every rank
-advances its own 2048^2 problem (independent problems, weak scaling); the
-timed region is bracketed by a barrier and device synchronisation and the
-time is the maximum over ranks.
+steps / time. With --gpus N (one process per GPU under torchrun) the problem
+is a 2048 x 2048N stack of the KH layer split along y, 2048^2 cells per
+rank (weak scaling): after every stage each rank exchanges its 3 edge rows
+with its neighbours (NCCL send/recv through the boundary hook) and every
+step's dt is the global CFL minimum (all-reduce MIN); --decomp replicas runs
+an independent 2048^2 problem per rank instead. The timed region is
+bracketed by a barrier and device synchronisation and the time is the
+maximum over ranks.
 
 --impl reference times the reference's own CPU implementation of the same
 step (the reference's hot-path sources compiled against the host shim,
@@ -51,19 +55,29 @@ def parse():
                     help="kh2d: the headline line; sedov3d and batch print their own lines")
     ap.add_argument("--solver", default="hllc", choices=["hllc", "rusanov"], help="batch workload solver")
     ap.add_argument("--fd-directions", type=int, default=64, help="adjoint workload: finite-difference checks")
+    ap.add_argument("--decomp", default="auto", choices=["auto", "slab", "replicas"],
+                    help="kh2d: one problem split along y with halo exchange (slab; auto = slab when --gpus > 1) "
+                         "or an independent problem per GPU (replicas)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
 
-def config(n, precision, world):
-    return {"workload": WORKLOAD if (n == N_CELLS_SIDE and precision == "fp64") else
-            f"kelvin_helmholtz_2d_{n}x{n}_weno5z_hllc_ssprk3_{precision}",
-            "grid": f"{n}x{n}", "ghost_cells": 3, "vars": 4, "reconstruction": "weno5z",
-            "riemann_solver": "hllc", "time_stepper": "ssprk3", "cfl": 0.4, "gamma": 5.0 / 3.0,
-            "boundaries": "periodic", "per_rank_problem": f"one {n}x{n} problem per GPU",
-            "parallelism": f"independent problems x{world}",
-            "l2": "inputs larger than L2 (state 135 MB; each step streams ~400 MB), no flush"}
+def config(n, precision, world, decomp="auto"):
+    c = {"workload": WORKLOAD if (n == N_CELLS_SIDE and precision == "fp64") else
+         f"kelvin_helmholtz_2d_{n}x{n}_weno5z_hllc_ssprk3_{precision}",
+         "grid": f"{n}x{n}", "ghost_cells": 3, "vars": 4, "reconstruction": "weno5z",
+         "riemann_solver": "hllc", "time_stepper": "ssprk3", "cfl": 0.4, "gamma": 5.0 / 3.0,
+         "boundaries": "periodic", "per_rank_problem": f"{n}x{n} cells per GPU",
+         "parallelism": "one GPU",
+         "l2": "inputs larger than L2 (state 135 MB; each step streams ~400 MB), no flush"}
+    if decomp == "slab" or (decomp == "auto" and world > 1):
+        c["grid"] = f"{n}x{n * world} (KH layer stacked {world}x in y)"
+        c["parallelism"] = (f"slab decomposition along y over {world} GPUs: ghost-row exchange after every stage "
+                            f"(NCCL send/recv), global dt by all-reduce MIN")
+    elif world > 1:
+        c["parallelism"] = f"independent {n}x{n} problems x{world}"
+    return c
 
 
 # ---------------------------------------------------------------------------
@@ -225,10 +239,31 @@ def run_ours(args):
     n = args.n
     p = P.kelvin_helmholtz_2d(n, seed=rank)
     cells = n * n
-    sim = HydroSim(p, precision=args.precision, device=dev)
-    sim.fill_bcs()
+    slab = None
+    use_slab = args.decomp == "slab" or (args.decomp == "auto" and world > 1)
+    if use_slab:
+        # one n x (n * world) periodic layer stack split along y: rank r owns
+        # rows [r n, (r + 1) n), a unit-square copy of the KH layer (continuous
+        # across slabs, since the layer is periodic in y); ghost rows come from
+        # the neighbours after every stage (NCCL point-to-point through the
+        # boundary hook) and dt is the global CFL minimum (all-reduce MIN)
+        from mosscap_b200.distributed import SlabSim
+        slab = SlabSim(p, rank, world, precision=args.precision, device=dev, is_slab=True)
+        sim = slab.sim
+        slab.fill_bcs()
+
+        def advance(k):
+            for _ in range(k):
+                slab.step()
+            return k
+    else:
+        sim = HydroSim(p, precision=args.precision, device=dev)
+        sim.fill_bcs()
+
+        def advance(k):
+            return len(sim.advance(k, log_dt=False)) if k else 0
     if args.warmup:
-        sim.advance(args.warmup, log_dt=False)
+        advance(args.warmup)
     stream = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
@@ -242,7 +277,7 @@ def run_ours(args):
     launches0 = sim.launch_count()
     sim.profile_stages(True)
     e0.record(stream)
-    steps_done = len(sim.advance(args.steps, log_dt=False)) if args.steps else 0
+    steps_done = advance(args.steps)
     e1.record(stream)
     barrier()
     clocks = sampler.stop()
@@ -281,8 +316,11 @@ def run_ours(args):
         t0 = time.perf_counter()
         for _ in range(K):
             sim.Q.copy_(host, non_blocking=True)
-            dt = sim.compute_dt()          # dt back on the host, like the reference hook
-            sim.time_step(dt)
+            if slab is not None:
+                slab.step()                # global dt read back on the host, then the step
+            else:
+                dt = sim.compute_dt()      # dt back on the host, like the reference hook
+                sim.time_step(dt)
             host.copy_(sim.Q, non_blocking=True)
             torch.cuda.synchronize(dev)
         barrier()
@@ -303,7 +341,7 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
-                "data": "synthetic", "config": config(n, args.precision, world), "roofline": roofline,
+                "data": "synthetic", "config": config(n, args.precision, world, args.decomp), "roofline": roofline,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
                 "status_flags": int(flags)}
         print(json.dumps(line), flush=True)
@@ -387,7 +425,7 @@ def run_adjoint(args):
     from mosscap_b200 import problems as P
     import ctypes
     from mosscap_b200 import capi
-    from mosscap_b200.adjoint import EulerSteps, _load_adjoint_symbols, _Runner, kh_initial_state, kh_vy, pad_periodic
+    from mosscap_b200.adjoint import EulerSteps, _Runner, kh_initial_state, kh_vy, pad_periodic
     n = args.n if args.n != N_CELLS_SIDE else 512
     steps = args.steps
     p = P.kelvin_helmholtz_2d(n, seed=0)
@@ -406,7 +444,6 @@ def run_adjoint(args):
     # cost: the C ABI calls on one mc_adjoint whose buffers a warm-up pass
     # allocated; forward = mc_adjoint_forward (K steps, checkpoints every 20),
     # adjoint = mc_adjoint_backward (segment recompute + reverse sweep)
-    _load_adjoint_symbols()
     runner = _Runner(p, p.gamma, 20)
     ng = p.ng
     with torch.no_grad():

@@ -284,6 +284,11 @@ mc_status mc_time_step_noalloc(const mc_grid* grid, const mc_scheme* scheme, dou
 /* Number of kernel launches issued by this context since it was created. */
 int64_t mc_launch_count(const mc_ctx* ctx);
 
+/* Diagnostic: out[i] = the reciprocal the adjoint's reverse sweep uses for
+ * x[i] (device arrays of n doubles), so that its error against IEEE 1/x can
+ * be measured. No counterpart in the reference. */
+mc_status mc_debug_reverse_reciprocal(const double* x, double* out, int64_t n, void* stream);
+
 /* Message of the last failed call on this thread (static storage). */
 const char* mc_last_error(void);
 

@@ -80,25 +80,10 @@ class _Runner:
         return g.value
 
 
-def _load_adjoint_symbols():
-    lib = capi.load()
-    vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
-    P = ctypes.POINTER
-    lib.mc_adjoint_create.argtypes = [P(capi.McGrid), P(capi.McScheme), i32, P(vp)]
-    lib.mc_adjoint_create.restype = i32
-    lib.mc_adjoint_destroy.argtypes = [vp]
-    lib.mc_adjoint_destroy.restype = i32
-    lib.mc_adjoint_forward.argtypes = [vp, vp, P(capi.McClock), i64, vp]
-    lib.mc_adjoint_forward.restype = i32
-    lib.mc_adjoint_backward.argtypes = [vp, vp, P(ctypes.c_double), vp]
-    lib.mc_adjoint_backward.restype = i32
-
-
 class EulerSteps(torch.autograd.Function):
     @staticmethod
     def forward(ctx, q0: torch.Tensor, gamma: torch.Tensor, problem: Problem, n_steps: int,
                 checkpoint_every: int = 20) -> torch.Tensor:
-        _load_adjoint_symbols()
         ng = problem.ng
         runner = _Runner(problem, float(gamma), checkpoint_every)
         qpad = pad_periodic(q0.detach().to(torch.float64), ng)

@@ -136,6 +136,16 @@ def load() -> ctypes.CDLL:
     lib.mc_time_step_noalloc.restype = i32
     lib.mc_launch_count.argtypes = [vp]
     lib.mc_launch_count.restype = i64
+    lib.mc_adjoint_create.argtypes = [P(McGrid), P(McScheme), i32, P(vp)]
+    lib.mc_adjoint_create.restype = i32
+    lib.mc_adjoint_destroy.argtypes = [vp]
+    lib.mc_adjoint_destroy.restype = i32
+    lib.mc_adjoint_forward.argtypes = [vp, vp, P(McClock), i64, vp]
+    lib.mc_adjoint_forward.restype = i32
+    lib.mc_adjoint_backward.argtypes = [vp, vp, P(d), vp]
+    lib.mc_adjoint_backward.restype = i32
+    lib.mc_debug_reverse_reciprocal.argtypes = [vp, vp, i64, vp]
+    lib.mc_debug_reverse_reciprocal.restype = i32
     if lib.mc_abi_version() != 1:
         raise RuntimeError("unexpected ABI version")
     _LIB = lib

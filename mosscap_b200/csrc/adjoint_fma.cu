@@ -37,20 +37,27 @@ using mc::StageParams;
 
 namespace {
 
-constexpr int kAT = 26;               // adjoint tile: 26 x 26 output cells
+// The adjoint tile is AT x AT output cells. A warp sweeps one line of the
+// tile with lane L on cell L - 3: cells -3 .. 28 are reconstructed, faces
+// -2 .. AT are solved and the stencil cotangents of cells -2 .. AT + 1 are
+// gathered into the AT own cells, so AT <= 26. kTile = 26 measured as fast
+// as 24 on the 512^2 adjoint (24 gives every warp 3 lines per pass, 26
+// gives two of the eight warps a fourth) with fewer halo cells per output.
+constexpr int kTile = 26;
 constexpr int kAH = 5;                // primitive halo (stencils of the reconstructions feeding the faces)
 constexpr int kMH = 3;                // cotangent halo
-constexpr int kAW = kAT + 2 * kAH;    // 36 stored rows / columns of primitives
-constexpr int kAP = kAW + 1;          // odd pitch
-constexpr int kMW = kAT + 2 * kMH;    // 32
-constexpr int kMP = kMW + 1;
-constexpr int kBP = kAT + 1;          // pitch of the tile's primitive cotangents
 constexpr int kAThreads = 256;
 constexpr int kAWarps = kAThreads / 32;
 
-size_t vjp_smem_bytes() {
-    return sizeof(double) * 4 * (size_t)(kAW * kAP + kMW * kMP + kAT * kBP);
-}
+template <int AT>
+struct VjpTile {
+    static constexpr int kAW = AT + 2 * kAH;  // stored rows / columns of primitives
+    static constexpr int kAP = kAW + 1;       // odd pitch
+    static constexpr int kMW = AT + 2 * kMH;  // stored rows / columns of cotangents
+    static constexpr int kMP = kMW + 1;
+    static constexpr int kBP = AT + 1;        // pitch of the tile's primitive cotangents
+    static size_t smem_bytes() { return sizeof(double) * 4 * (size_t)(kAW * kAP + kMW * kMP + AT * kBP); }
+};
 
 struct VjpParams {
     const double* q;        // stage input (padded layout, periodic ghosts)
@@ -96,21 +103,24 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
     return s;
 }
 
+template <int AT>
 __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
+    using TL = VjpTile<AT>;
+    constexpr int kAW = TL::kAW, kAP = TL::kAP, kMW = TL::kMW, kMP = TL::kMP, kBP = TL::kBP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* W = reinterpret_cast<double*>(smem_raw);   // [4][kAW][kAP]
     double* MU = W + 4 * kAW * kAP;                     // [4][kMW][kMP]
-    double* WB = MU + 4 * kMW * kMP;                    // [4][kAT][kBP]
+    double* WB = MU + 4 * kMW * kMP;                    // [4][AT][kBP]
     __shared__ double red[kAWarps];
-    const int x0 = blockIdx.x * kAT, y0 = blockIdx.y * kAT;
-    const int vw = min(kAT, p.nx - x0), vh = min(kAT, p.ny - y0);
+    const int x0 = blockIdx.x * AT, y0 = blockIdx.y * AT;
+    const int vw = min(AT, p.nx - x0), vh = min(AT, p.ny - y0);
     const double gamma = p.gamma;
     const mc::GasK K = mc::gas_constants(gamma);
 
     // primitives with a periodic cross-shaped halo of kAH cells
     {
-        constexpr int core = kAT * kAW;
-        constexpr int items = core + 2 * kAH * kAT;
+        constexpr int core = AT * kAW;
+        constexpr int items = core + 2 * kAH * AT;
         for (int it = threadIdx.x; it < items; it += kAThreads) {
             int tx, ty;
             if (it < core) {
@@ -118,9 +128,9 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
                 tx = it - ty * kAW - kAH;
             } else {
                 const int r = it - core;
-                const int hr = r / kAT;
-                tx = r - hr * kAT;
-                ty = hr < kAH ? hr - kAH : kAT + hr - kAH;
+                const int hr = r / AT;
+                tx = r - hr * AT;
+                ty = hr < kAH ? hr - kAH : AT + hr - kAH;
             }
             const int i = p.ng + wrap(x0 + tx, p.nx), j = p.ng + wrap(y0 + ty, p.ny);
             double q[4], w[4];
@@ -134,8 +144,8 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
                 W[(v * kAW + ty + kAH) * kAP + tx + kAH] = w[v];
             }
         }
-        constexpr int mcore = kAT * kMW;
-        constexpr int mitems = mcore + 2 * kMH * kAT;
+        constexpr int mcore = AT * kMW;
+        constexpr int mitems = mcore + 2 * kMH * AT;
         for (int it = threadIdx.x; it < mitems; it += kAThreads) {
             int tx, ty;
             if (it < mcore) {
@@ -143,9 +153,9 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
                 tx = it - ty * kMW - kMH;
             } else {
                 const int r = it - mcore;
-                const int hr = r / kAT;
-                tx = r - hr * kAT;
-                ty = hr < kMH ? hr - kMH : kAT + hr - kMH;
+                const int hr = r / AT;
+                tx = r - hr * AT;
+                ty = hr < kMH ? hr - kMH : AT + hr - kMH;
             }
             const int i = p.ng + wrap(x0 + tx, p.nx), j = p.ng + wrap(y0 + ty, p.ny);
 #pragma unroll
@@ -153,7 +163,7 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
                 MU[(v * kMW + ty + kMH) * kMP + tx + kMH] = p.mu[pidx(p, v, j, i)];
             }
         }
-        for (int it = threadIdx.x; it < 4 * kAT * kBP; it += kAThreads) {
+        for (int it = threadIdx.x; it < 4 * AT * kBP; it += kAThreads) {
             WB[it] = 0.0;
         }
     }
@@ -225,7 +235,7 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
                 const double g = __shfl_down_sync(0xffffffffu, sb[0], 2) + __shfl_down_sync(0xffffffffu, sb[1], 1) +
                                  sb[2] + __shfl_up_sync(0xffffffffu, sb[3], 1) + __shfl_up_sync(0xffffffffu, sb[4], 2);
                 if (own_cell) {
-                    double* dst = axis == 0 ? &WB[(v * kAT + line) * kBP + c] : &WB[(v * kAT + c) * kBP + line];
+                    double* dst = axis == 0 ? &WB[(v * AT + line) * kBP + c] : &WB[(v * AT + c) * kBP + line];
                     *dst += g;
                 }
             }
@@ -234,8 +244,8 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
     }
 
     // primitive cotangents -> conserved cotangents; write lam, acc
-    for (int it = threadIdx.x; it < kAT * kAT; it += kAThreads) {
-        const int ty = it / kAT, tx = it - ty * kAT;
+    for (int it = threadIdx.x; it < AT * AT; it += kAThreads) {
+        const int ty = it / AT, tx = it - ty * AT;
         if (tx >= vw || ty >= vh) {
             continue;
         }
@@ -244,7 +254,7 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             q[v] = p.q[pidx(p, v, j, i)];
-            wb[v] = WB[(v * kAT + ty) * kBP + tx];
+            wb[v] = WB[(v * AT + ty) * kBP + tx];
         }
         mc::prim_from_cons_vjp2(gamma, q, wb, qb, &gam);
 #pragma unroll
@@ -329,6 +339,12 @@ __global__ void dt_vjp_kernel(const double* q, int nx, int ng, int xc, int yc, d
     *gamma_bar += k * gb;
 }
 
+
+__global__ void reciprocal_kernel(const double* x, double* out, long long n) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        out[k] = mc::arcp(x[k]);
+    }
+}
 
 __global__ void zero_kernel(double* p, long long n) {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
@@ -474,8 +490,8 @@ mc_status vjp_stage(mc_adjoint* a, const double* q, const double* mu, double* la
     p.yc = a->grid.yc;
     p.part_gdt = a->part;
     p.part_gam = a->part + a->tiles;
-    const dim3 grid((a->nx + kAT - 1) / kAT, (a->ny + kAT - 1) / kAT);
-    stage_vjp_kernel<<<grid, kAThreads, vjp_smem_bytes(), s>>>(p);
+    const dim3 grid((a->nx + kTile - 1) / kTile, (a->ny + kTile - 1) / kTile);
+    stage_vjp_kernel<kTile><<<grid, kAThreads, VjpTile<kTile>::smem_bytes(), s>>>(p);
     MCA_CUDA(cudaGetLastError(), "stage vjp");
     reduce_stage_kernel<<<1, 256, 0, s>>>(a->part, a->part + a->tiles, a->tiles, coef_b / a->grid.dx, a->scal,
                                           a->scal + 1);
@@ -519,7 +535,7 @@ mc_status mc_adjoint_create(const mc_grid* grid, const mc_scheme* scheme, int32_
     a->ny = g.yc - 2 * g.ng;
     a->plane = (long long)g.xc * g.yc;
     a->state = 4 * (size_t)a->plane;
-    a->tiles = ((a->nx + kAT - 1) / kAT) * ((a->ny + kAT - 1) / kAT);
+    a->tiles = ((a->nx + kTile - 1) / kTile) * ((a->ny + kTile - 1) / kTile);
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void** p, size_t bytes) {
         if (e == cudaSuccess) {
@@ -542,7 +558,8 @@ mc_status mc_adjoint_create(const mc_grid* grid, const mc_scheme* scheme, int32_
     alloc((void**)&a->scal, sizeof(double) * 2);
     alloc((void**)&a->argmin, sizeof(int));
     if (e == cudaSuccess) {
-        e = cudaFuncSetAttribute(stage_vjp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vjp_smem_bytes());
+        e = cudaFuncSetAttribute(stage_vjp_kernel<kTile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)VjpTile<kTile>::smem_bytes());
     }
     if (e != cudaSuccess) {
         mc_adjoint_destroy(a);
@@ -682,6 +699,17 @@ mc_status mc_adjoint_backward(mc_adjoint* a, double* lambda, double* dgamma, voi
     if (dgamma) {
         MCA_CUDA(cudaMemcpyAsync(dgamma, a->scal + 1, sizeof(double), cudaMemcpyDeviceToHost, s), "dgamma");
         MCA_CUDA(cudaStreamSynchronize(s), "sync");
+    }
+    return MC_OK;
+}
+
+mc_status mc_debug_reverse_reciprocal(const double* x, double* out, int64_t n, void* stream) {
+    if (!x || !out || n < 0) {
+        return afail(MC_ERR_INVALID_ARGUMENT, "null argument or negative count");
+    }
+    if (n > 0) {
+        reciprocal_kernel<<<148 * 4, 256, 0, (cudaStream_t)stream>>>(x, out, n);
+        MCA_CUDA(cudaGetLastError(), "reciprocal");
     }
     return MC_OK;
 }

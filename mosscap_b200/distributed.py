@@ -99,13 +99,17 @@ class SlabSim:
     """This rank's slab of a 2D problem split along y over `world` ranks."""
 
     def __init__(self, problem: Problem, rank: int = 0, world: int = 1, precision: str = "fp64",
-                 device: Optional[torch.device] = None, group=None):
+                 device: Optional[torch.device] = None, group=None, is_slab: bool = False):
+        """problem: the global problem, whose rows are split over the ranks;
+        or, with is_slab, this rank's slab itself (its ny rows and their
+        ghost rows, the global problem's face kinds), so that no rank builds
+        the global state."""
         p = problem
-        if p.num_dim != 2 or p.ny % world != 0:
+        if p.num_dim != 2 or (not is_slab and p.ny % world != 0):
             raise ValueError("a 2D problem whose row count divides by the number of ranks")
         self.rank, self.world, self.group = rank, world, group
         self.ng = p.ng
-        self.ny = p.ny // world
+        self.ny = p.ny if is_slab else p.ny // world
         self.periodic_y = p.bc[2] == "periodic"
         bc = list(p.bc)
         if rank > 0 or self.periodic_y:
@@ -113,9 +117,13 @@ class SlabSim:
         if rank < world - 1 or self.periodic_y:
             bc[3] = "userfn"
         ng = p.ng
-        rows = slice(rank * self.ny, rank * self.ny + self.ny + 2 * ng)
-        local = replace(p, ny=self.ny, bc=tuple(bc), loc=(p.loc[0], p.loc[1] + rank * self.ny * p.dx, p.loc[2]),
-                        Q=np.ascontiguousarray(p.Q[:, :, rows, :]))
+        if is_slab:
+            local = replace(p, bc=tuple(bc))
+        else:
+            rows = slice(rank * self.ny, rank * self.ny + self.ny + 2 * ng)
+            local = replace(p, ny=self.ny, bc=tuple(bc),
+                            loc=(p.loc[0], p.loc[1] + rank * self.ny * p.dx, p.loc[2]),
+                            Q=np.ascontiguousarray(p.Q[:, :, rows, :]))
         self.problem = local
         self.sim = HydroSim(local, precision=precision, device=device)
         self._hook = capi.USER_BC_FN(self._fill_rows)

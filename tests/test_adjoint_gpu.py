@@ -111,3 +111,24 @@ def test_adjoint_checkpoint_interval_does_not_change_gradient(gpu_lib):
     _, g3, gg3 = _loss_and_grad(p, vy, p.gamma, rho_t, steps, 100)
     assert torch.equal(g1, g2) and torch.equal(g2, g3)
     assert gg1 == gg2 == gg3
+
+
+def test_reverse_reciprocal_error_bound(gpu_lib):
+    """The reciprocal of the reverse sweep (rcp.approx.ftz.f64 refined by two
+    Newton-Raphson steps) against IEEE 1/x: within 2 ulp over normal inputs of
+    either sign whose reciprocal is normal (every denominator the sweep
+    inverts is such a value)."""
+    import ctypes
+    from mosscap_b200 import capi
+    rng = np.random.default_rng(0)
+    n = 1 << 20
+    x = rng.uniform(1.0, 10.0, n) * 10.0 ** rng.uniform(-300.0, 300.0, n) * rng.choice([-1.0, 1.0], n)
+    x[:8] = [1.0, 2.0, 3.0, 1.0 / 3.0, 0.1, 1e-36, 1e20, 5.0 / 3.0 - 1.0]
+    xt = torch.tensor(x, device="cuda")
+    out = torch.empty_like(xt)
+    capi.check(gpu_lib.mc_debug_reverse_reciprocal(ctypes.c_void_p(xt.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                                   n, None), "mc_debug_reverse_reciprocal")
+    torch.cuda.synchronize()
+    ref = 1.0 / x
+    ulps = np.abs(out.cpu().numpy() - ref) / np.spacing(np.abs(ref))
+    assert ulps.max() <= 2.0, ulps.max()

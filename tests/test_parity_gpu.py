@@ -196,3 +196,37 @@ def test_slab_decomposition_single_rank(gpu_lib, oracle_port):
     dts = [s.step() for _ in range(8)]
     _assert_same(np.array(dts), ref_dts, "dt")
     _assert_same(s.sim.get_Q(), o.get_Q(), "state")
+
+
+def _rel_errors(a, ref):
+    d = np.abs(a - ref)
+    return float(d.sum() / np.abs(ref).sum()), float(d.max() / np.abs(ref).max())
+
+
+@pytest.mark.parametrize("n", [64, 128])
+def test_sedov_fp64_and_fp32_against_oracle(gpu_lib, oracle_port, n):
+    """3D Sedov at 64^3 and 128^3 to t = 0.05: the FP64 form is bit-exact
+    against the oracle (dt sequence and state); the FP32 form (its own dt
+    sequence from its FP64 state) stays within 1e-7 relative L1 and 1e-5
+    relative Linf in density. The errors are printed for the record."""
+    p = P.sedov_3d(n)
+    o = _oracle(oracle_port, p)
+    ref_dts = o.run(10 ** 6)
+    ref = o.get_Q()
+    out = {}
+    for precision in ("fp64", "fp32"):
+        sim = _sim(p, precision=precision)
+        sim.fill_bcs()
+        dts = sim.run(10 ** 6)
+        assert sim.time == o.time == 0.05
+        q = sim.get_Q()
+        if precision == "fp64":
+            _assert_same(dts, ref_dts, "dt")
+            _assert_same(q, ref, "state")
+        ng = p.ng
+        core = (slice(None), slice(ng, -ng), slice(ng, -ng), slice(ng, -ng))
+        out[precision] = _rel_errors(q[core][0], ref[core][0]) + (len(dts), len(ref_dts))
+        assert sim.status() == 0
+    print(f"sedov {n}^3 t=0.05 density (rel L1, rel Linf, steps, oracle steps):", out)
+    l1, linf = out["fp32"][:2]
+    assert l1 < 1e-7 and linf < 1e-5, out
