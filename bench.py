@@ -55,6 +55,7 @@ def parse():
                     help="kh2d: the headline line; sedov3d and batch print their own lines")
     ap.add_argument("--solver", default="hllc", choices=["hllc", "rusanov"], help="batch workload solver")
     ap.add_argument("--fd-directions", type=int, default=64, help="adjoint workload: finite-difference checks")
+    ap.add_argument("--problems", type=int, default=4096, help="batch workload: number of problems (half 1D, half 2D)")
     ap.add_argument("--decomp", default="auto", choices=["auto", "slab", "replicas"],
                     help="kh2d: one problem split along y with halo exchange (slab; auto = slab when --gpus > 1) "
                          "or an independent problem per GPU (replicas)")
@@ -391,7 +392,8 @@ def run_batch(args):
     import torch
     from mosscap_b200 import problems as P
     from mosscap_b200.hydro import BatchSim
-    probs = P.riemann_batch(seed=0, n1d=2048, n2d=2048, riemann_solver=args.solver)
+    half = max(args.problems // 2, 1)
+    probs = P.riemann_batch(seed=0, n1d=half, n2d=half, riemann_solver=args.solver)
     cells = sum(p.interior_cells for p in probs)
     b = BatchSim(probs, precision=args.precision)
     b.fill_bcs()
@@ -409,7 +411,7 @@ def run_batch(args):
     line = {"metric": METRIC, "value": updates / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / max(args.steps, 1), "higher_is_better": True,
             "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
-            "config": {"workload": f"riemann_batch_2048x1d_2048x2d_muscl_minmod_{args.solver}_rk2_{args.precision}",
+            "config": {"workload": f"riemann_batch_{half}x1d_{half}x2d_muscl_minmod_{args.solver}_rk2_{args.precision}",
                        "problems": len(probs), "interior_cells": cells, "schedule": sched},
             "problems_flagged": int((status != 0).sum())}
     print(json.dumps(line), flush=True)

@@ -147,6 +147,15 @@ mc_status mc_destroy(mc_ctx* ctx);
  * when any active face is MC_BC_USERFN. fn = NULL removes the hook. */
 mc_status mc_set_user_bc(mc_ctx* ctx, void (*fn)(void* user, double* Q, void* stream), void* user);
 
+/* Registers the gravity source term (setup_gravity,
+ * source/SourceTerms/Gravity.cpp:44-70; config keys sources.gravity.x/y/z):
+ * every stage adds dt * (0, rho g_x, rho g_y, rho g_z, m . g) to the hydro
+ * variables of each interior cell, evaluated from the stage's input state
+ * (Gravity.cpp:16-41 with the stage updates of source/TimeStepping.cpp).
+ * Components beyond num_dim are ignored. enabled = 0 removes it (the
+ * default: no source term, S = 0). */
+mc_status mc_set_gravity(mc_ctx* ctx, int32_t enabled, double gx, double gy, double gz);
+
 /* fill_bcs (source/Boundaries.hpp:121-149): fill every ghost cell of Q from
  * the interior for the built-in boundary kinds, x then y then z. */
 mc_status mc_fill_bcs(mc_ctx* ctx, double* Q, void* stream);

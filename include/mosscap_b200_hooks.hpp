@@ -10,8 +10,10 @@
 //
 // The state stays in Mosscap's own device array (sim.state.Q.data()); the
 // library owns only its two stage buffers. Requirements: a CUDA build of
-// Mosscap in double precision (fp_t = f64), the ideal EOS, no registered
-// source terms; fill_bcs at setup can stay Mosscap's own or use mc_fill_bcs.
+// Mosscap in double precision (fp_t = f64), the ideal EOS, no source term
+// other than gravity (whose vector install() must be given, since the
+// registered std::function does not expose it); fill_bcs at setup can stay
+// Mosscap's own or use mc_fill_bcs.
 #pragma once
 
 #include <memory>
@@ -72,10 +74,26 @@ Context make_context(const Sim& sim) {
     return Context(c, ContextDeleter{});
 }
 
-// Replace Simulation::time_step and Simulation::compute_dt.
+// Replace Simulation::time_step and Simulation::compute_dt. gravity: the
+// sources.gravity.{x,y,z} values of the configuration, required when the
+// Simulation registered the gravity source term (setup_gravity,
+// source/SourceTerms/Gravity.cpp:44-70).
 template <class Sim>
-Context install(Sim& sim) {
+Context install(Sim& sim, const double* gravity = nullptr) {
     Context ctx = make_context(sim);
+    bool has_gravity = false;
+    for (const auto& term : sim.compute_source_terms) {
+        if (term.name != "gravity") {
+            throw std::runtime_error("mosscap_b200: unsupported source term \"" + term.name + "\"");
+        }
+        has_gravity = true;
+    }
+    if (has_gravity) {
+        if (!gravity) {
+            throw std::runtime_error("mosscap_b200: the gravity source term needs its vector in install()");
+        }
+        check(mc_set_gravity(ctx.get(), 1, gravity[0], gravity[1], gravity[2]), "mc_set_gravity");
+    }
     sim.time_step = [ctx](Sim& s, auto dt) {
         check(mc_time_step(ctx.get(), s.state.Q.data(), double(dt), nullptr), "mc_time_step");
         s.dt = dt;

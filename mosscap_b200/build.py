@@ -74,7 +74,7 @@ def build(verbose: bool = False, jobs: int = 0) -> str:
     hdr = _headers_mtime()
     jobs = jobs or max(1, min(len(srcs), os.cpu_count() or 1))
     # the biggest translation units first
-    srcs.sort(key=lambda s: ("_d3_" not in s, "_d2_" not in s, s))
+    srcs.sort(key=lambda s: ("_d3_" not in s, "_d2_" not in s, "_src" in s, s))
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
         objs = list(ex.map(lambda s: _compile(s, hdr, verbose), srcs))
     if os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs):

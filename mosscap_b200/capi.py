@@ -134,6 +134,8 @@ def load() -> ctypes.CDLL:
     lib.mc_batch_schedule.restype = i32
     lib.mc_time_step_noalloc.argtypes = [P(McGrid), P(McScheme), vp, d, vp]
     lib.mc_time_step_noalloc.restype = i32
+    lib.mc_set_gravity.argtypes = [vp, i32, d, d, d]
+    lib.mc_set_gravity.restype = i32
     lib.mc_launch_count.argtypes = [vp]
     lib.mc_launch_count.restype = i64
     lib.mc_adjoint_create.argtypes = [P(McGrid), P(McScheme), i32, P(vp)]

@@ -34,6 +34,8 @@ struct mc_ctx {
     bool min_from_clock = false;  // last CFL minimum sits in blk->last_cfl_min
     void (*user_bc)(void*, double*, void*) = nullptr;
     void* user_bc_data = nullptr;
+    int gravity = 0;              // mc_set_gravity
+    double grav[3] = {0.0, 0.0, 0.0};
     // kernel timing (mc_profile_stages)
     bool profiling = false;
     struct Timed {
@@ -104,6 +106,10 @@ StageParams base_params(const mc_ctx* c) {
     p.dx = c->grid.dx;
     p.gamma = c->scheme.gamma;
     p.blk = c->blk;
+    p.gravity = c->gravity;
+    for (int a = 0; a < 3; ++a) {
+        p.grav[a] = c->grav[a];
+    }
     for (int f = 0; f < 6; ++f) {
         p.bc.kind[f] = c->grid.bc[f];
         for (int v = 0; v < mc::kMaxVars; ++v) {
@@ -144,6 +150,18 @@ cudaError_t launch_stage_kernel(mc_ctx* c, const StageParams& p, int pass, cudaS
     const bool f32 = c->scheme.precision == MC_PRECISION_FP32_COMPENSATED;
     const int r = c->scheme.reconstruction, l = c->scheme.slope_limiter, rs = c->scheme.riemann_solver;
     c->launches += 1;
+    if (p.gravity) {
+        if (nd == 1) {
+            return f32 ? mc::launch_stage_d1_fp32_src(p, r, l, rs, pass, s)
+                       : mc::launch_stage_d1_fp64_src(p, r, l, rs, pass, s);
+        }
+        if (nd == 2) {
+            return f32 ? mc::launch_stage_d2_fp32_src(p, r, l, rs, pass, s)
+                       : mc::launch_stage_d2_fp64_src(p, r, l, rs, pass, s);
+        }
+        return f32 ? mc::launch_stage_d3_fp32_src(p, r, l, rs, pass, s)
+                   : mc::launch_stage_d3_fp64_src(p, r, l, rs, pass, s);
+    }
     if (nd == 1) {
         return f32 ? mc::launch_stage_d1_fp32(p, r, l, rs, pass, s) : mc::launch_stage_d1_fp64(p, r, l, rs, pass, s);
     }
@@ -349,6 +367,17 @@ mc_status mc_set_user_bc(mc_ctx* c, void (*fn)(void* user, double* Q, void* stre
     }
     c->user_bc = fn;
     c->user_bc_data = user;
+    return MC_OK;
+}
+
+mc_status mc_set_gravity(mc_ctx* c, int32_t enabled, double gx, double gy, double gz) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    c->gravity = enabled ? 1 : 0;
+    c->grav[0] = enabled ? gx : 0.0;
+    c->grav[1] = enabled && c->grid.num_dim > 1 ? gy : 0.0;
+    c->grav[2] = enabled && c->grid.num_dim > 2 ? gz : 0.0;
     return MC_OK;
 }
 

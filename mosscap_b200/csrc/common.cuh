@@ -62,6 +62,8 @@ struct StageParams {
     int reset_min;                    // nonzero: reset blk->cfl_min_bits (a stage before the last)
     BcDesc bc;
     DeviceBlock* blk;
+    int gravity;                      // nonzero: the gravity source term is registered
+    double grav[3];                   // its acceleration (x, y, z)
 };
 
 constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;
@@ -77,6 +79,47 @@ __device__ __forceinline__ void maybe_reset_min(const StageParams& p) {
 
 __device__ __forceinline__ double stage_dt(const StageParams& p) {
     return p.dt_dev ? *p.dt_dev : p.dt;
+}
+
+// Source term times dt of the 2 + NDIM hydro variables of interior cell
+// (k, j, i), evaluated from the stage input as the reference does: every
+// stage zeroes S (source/SourceTerms.hpp:8-10) and the registered source
+// terms then add to it from the current state (:12-16); the only source term
+// of the reference, gravity (source/SourceTerms/Gravity.cpp:16-41), adds
+// rho g_a to each momentum and m_x g_x (+ m_y g_y (+ m_z g_z)) to the energy;
+// the stage update adds S dt (source/TimeStepping.cpp:60-66). SRC is false
+// in the kernels launched without a source term: S stays 0 and the result is
+// 0 * dt.
+template <int NDIM, bool SRC>
+__device__ __forceinline__ void source_dt(const StageParams& p, int k, int j, int i, double dt, double* sdt) {
+    constexpr int nh = 2 + NDIM;
+    if constexpr (!SRC) {
+#pragma unroll
+        for (int v = 0; v < nh; ++v) {
+            sdt[v] = 0.0 * dt;
+        }
+        return;
+    }
+    (void)p.gravity;
+    auto q = [&](int v) { return p.q_in[(((long long)v * p.zc + k) * p.yc + j) * (long long)p.xc + i]; };
+    const double rho = q(0);
+    double S[nh];
+    S[0] = 0.0;
+    double energy_update = q(1) * p.grav[0];
+    S[1] = 0.0 + rho * p.grav[0];
+    if constexpr (NDIM > 1) {
+        S[2] = 0.0 + rho * p.grav[1];
+        energy_update += q(2) * p.grav[1];
+    }
+    if constexpr (NDIM > 2) {
+        S[3] = 0.0 + rho * p.grav[2];
+        energy_update += q(3) * p.grav[2];
+    }
+    S[1 + NDIM] = 0.0 + energy_update;
+#pragma unroll
+    for (int v = 0; v < nh; ++v) {
+        sdt[v] = S[v] * dt;
+    }
 }
 
 // One SSPRK stage update of one variable; qu is the flux divergence already

@@ -15,6 +15,13 @@ cudaError_t launch_stage_d3_fp64(const StageParams& p, int rec, int lim, int rs,
 cudaError_t launch_stage_d1_fp32(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
 cudaError_t launch_stage_d2_fp32(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
 cudaError_t launch_stage_d3_fp32(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+// The same with the gravity source term (p.gravity set).
+cudaError_t launch_stage_d1_fp64_src(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d2_fp64_src(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d3_fp64_src(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d1_fp32_src(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d2_fp32_src(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d3_fp32_src(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
 
 // Ghost fill of Q from its interior (every built-in boundary kind).
 cudaError_t launch_fill_bcs(const StageParams& p, int ndim, cudaStream_t s);

@@ -18,6 +18,11 @@
 #ifndef MC_LAUNCH_NAME
 #error "MC_LAUNCH_NAME must be defined"
 #endif
+// MC_SRC 1: the variants with a registered source term (mc_set_gravity);
+// they compile in their own translation units.
+#ifndef MC_SRC
+#define MC_SRC 0
+#endif
 
 namespace mc {
 namespace {
@@ -41,7 +46,7 @@ template <int REC, int LIM, int RS>
 cudaError_t launch_one(const StageParams& p, int pass, cudaStream_t s) {
 #if MC_DIM == 1
     (void)pass;
-    auto k = stage1d_kernel<REC, LIM, RS, Real>;
+    auto k = stage1d_kernel<REC, LIM, RS, Real, MC_SRC>;
     const size_t sm = smem_bytes<1, REC, Real>(p.nvar);
     cudaError_t e = allow_smem(k, sm);
     if (e != cudaSuccess) {
@@ -50,7 +55,7 @@ cudaError_t launch_one(const StageParams& p, int pass, cudaStream_t s) {
     k<<<dim3(cdiv(p.nx, kWarps * kTile)), dim3(kThreads), sm, s>>>(p);
 #elif MC_DIM == 2
     (void)pass;
-    auto k = stage2d_kernel<2, REC, LIM, RS, Real>;
+    auto k = stage2d_kernel<2, REC, LIM, RS, Real, MC_SRC>;
     const size_t sm = smem_bytes<2, REC, Real>(p.nvar);
     cudaError_t e = allow_smem(k, sm);
     if (e != cudaSuccess) {
@@ -67,7 +72,7 @@ cudaError_t launch_one(const StageParams& p, int pass, cudaStream_t s) {
         }
         k<<<dim3(cdiv(p.nx, kTile), cdiv(p.ny, kTile), p.nz), dim3(kThreads), sm, s>>>(p);
     } else {
-        zsweep3d_kernel<REC, LIM, RS, Real>
+        zsweep3d_kernel<REC, LIM, RS, Real, MC_SRC>
             <<<dim3(cdiv(p.nx, kZBlockX), cdiv(p.ny, kZBlockY), cdiv(p.nz, kZChunk)), dim3(kZBlockX, kZBlockY), 0,
                s>>>(p);
     }

@@ -1,0 +1,7 @@
+// Stage-kernel launchers, 1D, FP32 (FP32 compute form), with the gravity
+// source term registered.
+#define MC_DIM 1
+#define MC_REAL float
+#define MC_SRC 1
+#define MC_LAUNCH_NAME launch_stage_d1_fp32_src
+#include "launch_impl.cuh"

@@ -274,7 +274,7 @@ __host__ __device__ constexpr int seg1d_window() {
     return kTile + 2 * halo_of<REC>();
 }
 
-template <int REC, int LIM, int RS, class T>
+template <int REC, int LIM, int RS, class T, bool SRC = false>
 __device__ __forceinline__ void segment1d(const StageParams& p, int x0, T* W, double& dtmin, unsigned& flags) {
     constexpr int NDIM = 1;
     constexpr int nh = 3;
@@ -304,13 +304,15 @@ __device__ __forceinline__ void segment1d(const StageParams& p, int x0, T* W, do
             qn[v] = 0.0;
         }
         const bool old = combo_reads_old(p.combo);
+        double sdt[nh];
+        source_dt<1, SRC>(p, 0, 0, i, dt, sdt);
 #pragma unroll
         for (int v = 0; v < nh; ++v) {
             double qu = 0.0;
             qu += double(d[v]);
             qu *= dtdx;
             const long long id = qidx(p, v, 0, 0, i);
-            qn[v] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0 * dt);
+            qn[v] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, sdt[v]);
         }
         for (int t = 0; t < p.ntracer; ++t) {
             double qu = 0.0;
@@ -324,7 +326,7 @@ __device__ __forceinline__ void segment1d(const StageParams& p, int x0, T* W, do
 }
 
 // 1D stage kernel: warp w of CTA b updates segment b * kWarps + w.
-template <int REC, int LIM, int RS, class T>
+template <int REC, int LIM, int RS, class T, bool SRC = false>
 __global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
     if (p.dt_dev && p.blk->done) {
         return;
@@ -339,7 +341,7 @@ __global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
     unsigned flags = 0;
     const int x0 = (blockIdx.x * kWarps + warp) * kTile;
     if (x0 < p.nx) {
-        segment1d<REC, LIM, RS, T>(p, x0, W, dtmin, flags);
+        segment1d<REC, LIM, RS, T, SRC>(p, x0, W, dtmin, flags);
     }
     block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
 }
@@ -351,7 +353,7 @@ __global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
 // One CTA updates tile (bx, by) of a 2D problem, or of z plane bz in the 3D
 // plane pass. smem holds nvar x (WY x P) primitives and nvar x (TY x PY)
 // y divergences. Contains CTA-wide barriers: every thread of the CTA calls it.
-template <int NDIM, int REC, int LIM, int RS, class T>
+template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false>
 __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int bz, T* smem, double& dtmin,
                                        unsigned& flags) {
     constexpr int nh = 2 + NDIM;
@@ -448,6 +450,8 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
                 for (int v = 0; v < kMaxVars; ++v) {
                     qn[v] = 0.0;
                 }
+                double sdt[nh];
+                source_dt<NDIM, SRC>(p, 0, j, i, dt, sdt);
 #pragma unroll
                 for (int v = 0; v < nh; ++v) {
                     double qu = 0.0;
@@ -455,7 +459,7 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
                     qu += double(dfy[v * YV]);
                     qu *= dtdx;
                     const long long id = qidx(p, v, 0, j, i);
-                    qn[v] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0 * dt);
+                    qn[v] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, sdt[v]);
                 }
                 for (int t = 0; t < ntr; ++t) {
                     double qu = 0.0;
@@ -472,7 +476,7 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
     }
 }
 
-template <int NDIM, int REC, int LIM, int RS, class T>
+template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : kMinBlocks2d)
     stage2d_kernel(StageParams p) {
     if (p.dt_dev && p.blk->done) {
@@ -484,7 +488,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : k
     __shared__ unsigned red_u[kWarps];
     double dtmin = __longlong_as_double(0x7ff0000000000000ll);
     unsigned flags = 0;
-    tile2d<NDIM, REC, LIM, RS, T>(p, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<T*>(smem_raw), dtmin,
+    tile2d<NDIM, REC, LIM, RS, T, SRC>(p, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<T*>(smem_raw), dtmin,
                                   flags);
     block_publish(dtmin, flags, NDIM != 3 && p.last != 0, p.blk, red_d, red_u);
 }
@@ -498,7 +502,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : k
 constexpr int kZChunk = 32;
 constexpr int kZBlockX = 32, kZBlockY = 4;
 
-template <int REC, int LIM, int RS, class T>
+template <int REC, int LIM, int RS, class T, bool SRC = false>
 __global__ void __launch_bounds__(kZBlockX* kZBlockY) zsweep3d_kernel(StageParams p) {
     if (p.dt_dev && p.blk->done) {
         return;
@@ -593,15 +597,16 @@ __global__ void __launch_bounds__(kZBlockX* kZBlockY) zsweep3d_kernel(StageParam
             for (int v = 0; v < kMaxVars; ++v) {
                 qn[v] = 0.0;
             }
+            double sdt[nh];
+            source_dt<NDIM, SRC>(p, kk, j, i, dt, sdt);
 #pragma unroll
             for (int v = 0; v < nh; ++v) {
                 double qu = p.dqxy[v * cells + o];
                 qu += double(f_prev[v] - f_cur[v]);
                 qu *= dtdx;
-                const double src = 0.0 * dt;
                 const long long id = qidx(p, v, kk, j, i);
                 const double qo = combo_reads_old(p.combo) ? p.q_old[id] : 0.0;
-                qn[v] = combine(p.combo, qo, p.q_in[id], qu, src);
+                qn[v] = combine(p.combo, qo, p.q_in[id], qu, sdt[v]);
             }
             dtmin = smin(write_cell<NDIM>(p, i, j, kk, qn, p.last != 0, &flags), dtmin);
 #pragma unroll

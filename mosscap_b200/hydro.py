@@ -68,6 +68,9 @@ class HydroSim:
         with torch.cuda.device(self.device):
             capi.check(self.lib.mc_create(ctypes.byref(g), ctypes.byref(s), ctypes.byref(h)), "mc_create")
         self.ctx = h
+        if p.gravity is not None:
+            gx, gy, gz = (float(x) for x in p.gravity)
+            capi.check(self.lib.mc_set_gravity(h, 1, gx, gy, gz), "mc_set_gravity")
         q = Q if Q is not None else p.Q
         if q is None:
             raise ValueError("no initial state")

@@ -40,6 +40,9 @@ class Problem:
     max_cfl: float = 0.8
     max_time: float = 1.0
     output_delta: float = 0.1
+    # acceleration of the gravity source term (sources.gravity.x/y/z of the
+    # reference's configuration); None: no source term
+    gravity: Optional[Tuple[float, float, float]] = None
     Q: Optional[np.ndarray] = field(default=None, repr=False)
 
     @property

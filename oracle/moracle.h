@@ -65,6 +65,10 @@ double moracle_get_time(void* sim);
 /* Sets the clock: current time and the time of the previous output. */
 void moracle_set_clock(void* sim, double time, double prev_output_time);
 void moracle_set_num_threads(int n);
+/* Registers the gravity source term (setup_gravity,
+ * source/SourceTerms/Gravity.cpp:44-70) with acceleration (gx, gy, gz);
+ * enabled = 0 leaves the simulation without source terms. */
+void moracle_set_gravity(void* sim, int enabled, double gx, double gy, double gz);
 
 #ifdef __cplusplus
 }

@@ -36,6 +36,8 @@ typedef struct {
     double *Q, *W, *RL, *RR, *F[3], *Qold;
     double time, prev_output_time;
     long long step;
+    int gravity;
+    double grav[3];
 } osim;
 
 /* std::min / std::max semantics (first argument wins ties and NaN compares). */
@@ -529,10 +531,36 @@ static void fill_bcs(osim* s) {
 
 /* ---- TimeStepping.cpp ------------------------------------------------------ */
 
+/* zero_source_terms + compute_source_terms (source/SourceTerms.hpp:8-16)
+ * for one cell: S = 0, then the gravity source term if registered
+ * (source/SourceTerms/Gravity.cpp:16-41): S(mom_a) += rho g_a,
+ * S(E) += m_x g_x (+ m_y g_y (+ m_z g_z)). Computed from the stage input
+ * before the cell is updated, as the reference's separate kernel is. */
+static void cell_sources(const osim* s, int k, int j, int i, double* S) {
+    for (int v = 0; v < s->nhydro; ++v) {
+        S[v] = 0.0;
+    }
+    if (!s->gravity) {
+        return;
+    }
+    const double rho = s->Q[at(s, 0, k, j, i)];
+    S[1] += rho * s->grav[0];
+    double energy_update = s->Q[at(s, 1, k, j, i)] * s->grav[0];
+    if (s->ndim > 1) {
+        S[2] += rho * s->grav[1];
+        energy_update += s->Q[at(s, 2, k, j, i)] * s->grav[1];
+    }
+    if (s->ndim > 2) {
+        S[3] += rho * s->grav[2];
+        energy_update += s->Q[at(s, 3, k, j, i)] * s->grav[2];
+    }
+    S[1 + s->ndim] += energy_update;
+}
+
 /* integrate_flux + the stage updates, source/TimeStepping.cpp:10-35 and the
  * stage lambdas of rk2 (:60-67, :80-87), ssprk3 (:137-144, :157-164,
- * :177-184) and ssprk4 (:234-241, :254-261, :274-281, :294-301). With no
- * source terms registered S is zero, so the source is 0.0 * dt. */
+ * :177-184) and ssprk4 (:234-241, :254-261, :274-281, :294-301); the source
+ * of hydro variable v is S(v) * dt. */
 static void integrate(osim* s, int stepper, int stage, double dt) {
     const range3 r = interior_range(s);
     const int nz = r.n[2], ny = r.n[1], nx = r.n[0];
@@ -544,6 +572,8 @@ static void integrate(osim* s, int stepper, int stage, double dt) {
                 const int k = nz == 1 ? ki : ki + ng;
                 const int j = ny == 1 ? ji : ji + ng;
                 const int i = ii + ng;
+                double S[5];
+                cell_sources(s, k, j, i, S);
                 for (int v = 0; v < s->nvar; ++v) {
                     const long long id = at(s, v, k, j, i);
                     double qu = 0.0;
@@ -557,7 +587,7 @@ static void integrate(osim* s, int stepper, int stage, double dt) {
                     qu *= dt / s->c.dx;
                     double source = 0.0;
                     if (v < s->nhydro) {
-                        source = 0.0 * dt;
+                        source = S[v] * dt;
                     }
                     double* Q = s->Q;
                     const double* Qo = s->Qold;
@@ -708,6 +738,14 @@ double moracle_get_time(void* p) { return ((osim*)p)->time; }
 void moracle_set_clock(void* p, double time, double prev_output_time) {
     ((osim*)p)->time = time;
     ((osim*)p)->prev_output_time = prev_output_time;
+}
+
+void moracle_set_gravity(void* p, int enabled, double gx, double gy, double gz) {
+    osim* s = (osim*)p;
+    s->gravity = enabled ? 1 : 0;
+    s->grav[0] = gx;
+    s->grav[1] = gy;
+    s->grav[2] = gz;
 }
 
 void moracle_set_num_threads(int n) {

@@ -95,6 +95,7 @@ def load(kind: str) -> ctypes.CDLL:
     lib.moracle_get_time.restype = d
     lib.moracle_set_clock.argtypes = [vp, d, d]
     lib.moracle_set_num_threads.argtypes = [ctypes.c_int]
+    lib.moracle_set_gravity.argtypes = [vp, ctypes.c_int, d, d, d]
     _LIBS[kind] = lib
     return lib
 
@@ -223,3 +224,11 @@ class OracleSim:
 
     def set_clock(self, time: float, prev_output_time: float) -> None:
         self.lib.moracle_set_clock(self.h, time, prev_output_time)
+
+    def set_gravity(self, g) -> None:
+        """Register the gravity source term with acceleration g = (gx, gy, gz);
+        None removes it."""
+        if g is None:
+            self.lib.moracle_set_gravity(self.h, 0, 0.0, 0.0, 0.0)
+        else:
+            self.lib.moracle_set_gravity(self.h, 1, float(g[0]), float(g[1]), float(g[2]))

@@ -13,6 +13,8 @@
 #include "TimeStepping.hpp"
 #include "Boundaries.hpp"
 #include "SourceTerms.hpp"
+#include "SourceTerms/Gravity.hpp"
+#include "yaml-cpp/yaml.h"
 
 #include <limits>
 #include <new>
@@ -196,6 +198,22 @@ double moracle_get_time(void* p) {
 void moracle_set_clock(void* p, double time, double prev_output_time) {
     S(p).time = time;
     S(p).out_cfg.prev_output_time = prev_output_time;
+}
+
+void moracle_set_gravity(void* p, int enabled, double gx, double gy, double gz) {
+    // the reference's own registration, with the configuration
+    // sources.gravity.{x,y,z} built in code
+    auto& sim = S(p);
+    sim.compute_source_terms.clear();
+    if (!enabled) {
+        return;
+    }
+    YAML::Node cfg;
+    YAML::Node g = cfg.child("sources").child("gravity");
+    g.child("x").set(gx);
+    g.child("y").set(gy);
+    g.child("z").set(gz);
+    Mosscap::setup_gravity(sim, cfg);
 }
 
 void moracle_set_num_threads(int n) {

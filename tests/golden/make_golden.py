@@ -10,8 +10,9 @@ synthetic inputs and records:
   for the three headline workloads at fixture size (Sod 1D at full size, KH 2D
   at 64^2, Sedov 3D at 12^3);
 * ``sweep.json`` -- for every reconstruction x limiter x Riemann solver x
-  stepper on small 1D / 2D / 3D grids with mixed boundary kinds, the SHA-256
-  of the input and of the final state and the dt sequence (bit patterns).
+  stepper on small 1D / 2D / 3D grids with mixed boundary kinds, and for the
+  gravity source term with every stepper, the SHA-256 of the input and of the
+  final state and the dt sequence (bit patterns).
 
 Run from the repository root:  python tests/golden/make_golden.py
 """
@@ -44,6 +45,8 @@ def cfg_of(p: P.Problem) -> OracleConfig:
 
 def run_case(p: P.Problem, steps: int, kind: str = "reference"):
     s = OracleSim(cfg_of(p), kind)
+    if p.gravity is not None:
+        s.set_gravity(p.gravity)
     s.set_Q(p.Q)
     s.fill_bcs()
     q0 = s.get_Q()
@@ -87,6 +90,18 @@ def sweep_cases():
                           reconstruction=rec, slope_limiter=lim, riemann_solver=rs, time_stepper=st,
                           gamma=1.4, max_cfl=0.6, max_time=0.04, output_delta=0.015, Q=q)
             out.append((p.name, p, 6, seed))
+    # the gravity source term (source/SourceTerms/Gravity.cpp) with every
+    # stepper in 1D / 2D / 3D
+    for ndim, st in itertools.product((1, 2, 3), ("rk2", "ssprk3", "ssprk4")):
+        n = SWEEP_N[ndim]
+        seed = 5000 + 10 * ndim + ("rk2", "ssprk3", "ssprk4").index(st)
+        rec, lim = [("muscl", "vanleer"), ("ppm", "monotonizedcentral"), ("weno5z", "monotonizedcentral")][ndim - 1]
+        q = P.random_state(ndim, n, n, n, ng=3, seed=seed)
+        p = P.Problem(f"gravity_{ndim}d_{rec}_{st}", ndim, n, n if ndim > 1 else 1, n if ndim > 2 else 1, ng=3,
+                      dx=1.0 / n, bc=SWEEP_BCS[ndim], reconstruction=rec, slope_limiter=lim, riemann_solver="hllc",
+                      time_stepper=st, gamma=1.4, max_cfl=0.6, max_time=0.04, output_delta=0.015,
+                      gravity=(-1.5, 0.75, -0.5), Q=q)
+        out.append((p.name, p, 6, seed))
     return out
 
 

@@ -18,6 +18,8 @@ def _sha(a):
 
 def _run(O, kind, p, steps):
     s = O.OracleSim(O.OracleConfig(**p.scheme_fields()), kind)
+    if p.gravity is not None:
+        s.set_gravity(p.gravity)
     s.set_Q(p.Q)
     s.fill_bcs()
     q0 = s.get_Q()
@@ -58,7 +60,7 @@ def test_sweep_fixture(kind, request):
         assert [int(x) for x in _bits(dts)] == g["dt_bits"], name
         assert _sha(q1) == g["q1_sha256"], name
         n += 1
-    assert n == len(gold) == 216
+    assert n == len(gold) == 225
 
 
 def test_constant_boundaries_port_vs_reference(oracle_port, oracle_ref):
