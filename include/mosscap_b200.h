@@ -228,10 +228,12 @@ mc_status mc_batch_create(const mc_batch_problem* problems, int32_t n, const mc_
 mc_status mc_batch_destroy(mc_batch* batch);
 /* Fill every problem's ghost cells (fill_bcs per problem). */
 mc_status mc_batch_fill_bcs(mc_batch* batch, double* pool, void* stream);
-/* Autotuner: times the stage kernel on this pool for every candidate
- * schedule (persistent grid size, static or dynamic work distribution, 1D
- * segments per warp task) with CUDA events and keeps the fastest. Leaves the
- * pool unchanged. Waits for the stream. */
+/* Autotuner: times the stage kernels (one launch over the 2D problems'
+ * tiles, one over the 1D problems' warp tasks) on this pool for every
+ * candidate schedule (persistent grid size, static or dynamic work
+ * distribution; for the 1D launch also the segments per warp task) with CUDA
+ * events and keeps the fastest of each. Leaves the pool unchanged. Waits for
+ * the stream. */
 mc_status mc_batch_tune(mc_batch* batch, double* pool, void* stream);
 /* Up to `steps` steps of every unfinished problem, each with its own dt, on
  * the device (graph replay). The first call computes every problem's first
@@ -240,7 +242,8 @@ mc_status mc_batch_advance(mc_batch* batch, double* pool, int64_t steps, void* s
 /* Per-problem clocks, steps taken and MC_FLAG_* status (NULL to skip any).
  * Waits for the stream. */
 mc_status mc_batch_clocks(mc_batch* batch, mc_clock* clocks, int64_t* steps, uint32_t* status, void* stream);
-/* The schedule in use: grid size in CTAs, 1 if dynamic, 1D segments per warp task. */
+/* The schedule in use: grid size in CTAs and 1 if dynamic, of the launch over
+ * the 2D tiles; 1D segments per warp task. */
 mc_status mc_batch_schedule(const mc_batch* batch, int32_t* grid, int32_t* dynamic, int32_t* segs_per_task);
 
 /* ---- Discrete adjoint --------------------------------------------------------

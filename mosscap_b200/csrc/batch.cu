@@ -30,28 +30,34 @@ struct mc_batch {
     std::vector<long long> cells;        // cells per problem (ghosts included) for ordering
     StageParams* d_params = nullptr;
     long long* d_offsets = nullptr;
+    StageParams* d_stage = nullptr;      // per stage, every problem's parameters bound to a pool (bind_stages)
+    const double* stage_pool = nullptr;  // the pool d_stage is bound to
     DeviceBlock* d_blocks = nullptr;
     BatchItem2d* d_items2d = nullptr;
     int n2d = 0;
     BatchTask1d* d_tasks1d = nullptr;
     int ntasks1d = 0;
     int tasks_segs = 0;                  // segments per task the 1D list was built with
-    int* d_counters = nullptr;           // one work counter per stage
+    int* d_counters = nullptr;           // one work counter per stage and part (kCounters)
     double* buf_a = nullptr;
     double* buf_b = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     cudaGraphExec_t graph = nullptr;
     const double* graph_pool = nullptr;
-    int graph_key[3] = {0, 0, 0};
+    int graph_key[5] = {0, 0, 0, 0, 0};
     bool clocks_ready = false;
     const double* clocks_pool = nullptr;
-    // schedule
+    // schedule: the 2D-tile launch (grid, dynamic), the 1D launch (grid1d,
+    // dynamic1d, segs = 30-cell segments per warp task)
     int grid = 0;
     int dynamic = 1;
+    int grid1d = 0;
+    int dynamic1d = 1;
     int segs = 2;
     int sms = 148;
-    int occupancy = 1;
+    int occupancy = 1;     // resident CTAs per SM of the 2D-tile kernel
+    int occupancy1d = 1;   // and of the 1D kernel
 };
 
 namespace {
@@ -59,6 +65,8 @@ namespace {
 inline int cdiv(long long a, long long b) {
     return (int)((a + b - 1) / b);
 }
+
+constexpr int kCounters = 8;  // 4 stages x 2 parts
 
 mc_status bfail(mc_status s, const std::string& msg) {
     mc::set_last_error(msg.c_str());
@@ -135,7 +143,7 @@ __global__ void __launch_bounds__(256) batch_cfl_kernel(const StageParams* probs
 __global__ void batch_clock_kernel(DeviceBlock* blocks, int n, int first, int* counters) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < kCounters; ++c) {
             counters[c] = 0;
         }
     }
@@ -179,11 +187,12 @@ mc_status validate_problem(const mc_batch_problem& pr, const mc_scheme& s, int64
     return MC_OK;
 }
 
-cudaError_t launch_stage(const mc_batch* b, const BatchStageParams& bp, int grid, cudaStream_t s, int* occ) {
+cudaError_t launch_stage(const mc_batch* b, const BatchStageParams& bp, int part, int grid, cudaStream_t s,
+                         int* occ) {
     const bool f32 = b->scheme.precision == MC_PRECISION_FP32_COMPENSATED;
     const int r = b->scheme.reconstruction, l = b->scheme.slope_limiter, rs = b->scheme.riemann_solver;
-    return f32 ? mc::launch_batch_stage_fp32(bp, r, l, rs, grid, s, occ)
-               : mc::launch_batch_stage_fp64(bp, r, l, rs, grid, s, occ);
+    return f32 ? mc::launch_batch_stage_fp32(bp, r, l, rs, part, grid, s, occ)
+               : mc::launch_batch_stage_fp64(bp, r, l, rs, part, grid, s, occ);
 }
 
 // 1D task list: consecutive groups of `segs` 30-cell segments per problem,
@@ -218,23 +227,46 @@ mc_status build_tasks(mc_batch* b, int segs) {
     return MC_OK;
 }
 
-BatchStageParams stage_params(const mc_batch* b, const double* pool, int in, int old_, int out, int combo, int last,
-                              int dynamic, int* counter) {
+// Bind every problem's parameters to `pool` for each stage of the plan:
+// state pointers (input, step-start state, output), the stage combination
+// and the last-stage flag, so that the kernels read them in place.
+mc_status bind_stages(mc_batch* b, const double* pool) {
+    if (b->stage_pool == pool) {
+        return MC_OK;
+    }
     const double* bases[3] = {pool, b->buf_a, b->buf_b};
+    const Plan pl = plan_for(b->scheme.time_stepper);
+    std::vector<StageParams> tab((size_t)pl.n * b->n);
+    for (int st = 0; st < pl.n; ++st) {
+        for (int i = 0; i < b->n; ++i) {
+            StageParams q = b->params[i];
+            const int64_t off = b->problems[i].offset;
+            q.q_in = bases[pl.in[st]] + off;
+            q.q_old = pool + off;
+            q.q_out = const_cast<double*>(bases[pl.out[st]]) + off;
+            q.combo = pl.combo[st];
+            q.last = st == pl.n - 1;
+            q.reset_min = 0;
+            tab[(size_t)st * b->n + i] = q;
+        }
+    }
+    // earlier steps on the batch's stream may still read the old binding
+    MCB_CUDA(cudaStreamSynchronize(b->stream), "sync");
+    MCB_CUDA(cudaMemcpy(b->d_stage, tab.data(), sizeof(StageParams) * tab.size(), cudaMemcpyHostToDevice),
+             "stage parameters");
+    b->stage_pool = pool;
+    return MC_OK;
+}
+
+BatchStageParams stage_params(const mc_batch* b, int part, int st, int dynamic, int* counter) {
     BatchStageParams bp;
     std::memset(&bp, 0, sizeof(bp));
-    bp.probs = b->d_params;
-    bp.offsets = b->d_offsets;
+    bp.probs = b->d_stage + (size_t)st * b->n;
     bp.items2d = b->d_items2d;
     bp.n2d = b->n2d;
     bp.tasks1d = b->d_tasks1d;
     bp.ntasks1d = b->ntasks1d;
-    bp.n_items = b->n2d + cdiv(b->ntasks1d, mc::kWarps);
-    bp.in_base = bases[in];
-    bp.old_base = bases[old_];
-    bp.out_base = const_cast<double*>(bases[out]);
-    bp.combo = combo;
-    bp.last = last;
+    bp.n_items = part == mc::kPart2d ? b->n2d : cdiv(b->ntasks1d, mc::kWarps);
     bp.dynamic = dynamic;
     bp.counter = counter;
     return bp;
@@ -245,9 +277,14 @@ BatchStageParams stage_params(const mc_batch* b, const double* pool, int in, int
 mc_status enqueue_step(mc_batch* b, double* pool, cudaStream_t s) {
     const Plan pl = plan_for(b->scheme.time_stepper);
     for (int st = 0; st < pl.n; ++st) {
-        const BatchStageParams bp = stage_params(b, pool, pl.in[st], 0, pl.out[st], pl.combo[st],
-                                                 st == pl.n - 1, b->dynamic, b->d_counters + st);
-        MCB_CUDA(launch_stage(b, bp, b->grid, s, nullptr), "batch stage");
+        if (b->n2d > 0) {
+            const BatchStageParams bp = stage_params(b, mc::kPart2d, st, b->dynamic, b->d_counters + 2 * st);
+            MCB_CUDA(launch_stage(b, bp, mc::kPart2d, b->grid, s, nullptr), "batch stage");
+        }
+        if (b->ntasks1d > 0) {
+            const BatchStageParams bp = stage_params(b, mc::kPart1d, st, b->dynamic1d, b->d_counters + 2 * st + 1);
+            MCB_CUDA(launch_stage(b, bp, mc::kPart1d, b->grid1d, s, nullptr), "batch stage");
+        }
     }
     batch_clock_kernel<<<cdiv(b->n, 256), 256, 0, s>>>(b->d_blocks, b->n, 0, b->d_counters);
     MCB_CUDA(cudaGetLastError(), "batch clock");
@@ -281,8 +318,8 @@ mc_status init_clocks(mc_batch* b, double* pool, cudaStream_t s) {
 }
 
 mc_status ensure_graph(mc_batch* b, double* pool) {
-    const int key[3] = {b->grid, b->dynamic, b->segs};
-    if (b->graph && b->graph_pool == pool && std::equal(key, key + 3, b->graph_key)) {
+    const int key[5] = {b->grid, b->dynamic, b->segs, b->grid1d, b->dynamic1d};
+    if (b->graph && b->graph_pool == pool && std::equal(key, key + 5, b->graph_key)) {
         return MC_OK;
     }
     if (b->graph) {
@@ -292,10 +329,15 @@ mc_status ensure_graph(mc_batch* b, double* pool) {
     if (mc_status st = build_tasks(b, b->segs)) {
         return st;
     }
+    if (mc_status st = bind_stages(b, pool)) {
+        return st;
+    }
     // kernel attributes are set outside the capture
-    int occ = 0;
-    const BatchStageParams probe = stage_params(b, pool, 0, 0, 1, mc::kAdd, 0, 0, b->d_counters);
-    MCB_CUDA(launch_stage(b, probe, 1, b->stream, &occ), "occupancy");
+    for (int part : {mc::kPart2d, mc::kPart1d}) {
+        int occ = 0;
+        const BatchStageParams probe = stage_params(b, part, 0, 0, b->d_counters);
+        MCB_CUDA(launch_stage(b, probe, part, 1, b->stream, &occ), "occupancy");
+    }
     cudaGraph_t g = nullptr;
     MCB_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "capture");
     mc_status st = enqueue_step(b, pool, b->stream);
@@ -311,7 +353,7 @@ mc_status ensure_graph(mc_batch* b, double* pool) {
     cudaGraphDestroy(g);
     MCB_CUDA(e, "instantiate");
     b->graph_pool = pool;
-    std::copy(key, key + 3, b->graph_key);
+    std::copy(key, key + 5, b->graph_key);
     return MC_OK;
 }
 
@@ -357,8 +399,9 @@ mc_status mc_batch_create(const mc_batch_problem* problems, int32_t n, const mc_
     alloc((void**)&b->buf_b, sizeof(double) * (size_t)pool_doubles);
     alloc((void**)&b->d_params, sizeof(StageParams) * n);
     alloc((void**)&b->d_offsets, sizeof(long long) * n);
+    alloc((void**)&b->d_stage, sizeof(StageParams) * 4 * (size_t)n);
     alloc((void**)&b->d_blocks, sizeof(DeviceBlock) * n);
-    alloc((void**)&b->d_counters, sizeof(int) * 4);
+    alloc((void**)&b->d_counters, sizeof(int) * kCounters);
     if (e == cudaSuccess) {
         e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     }
@@ -429,7 +472,7 @@ mc_status mc_batch_create(const mc_batch_problem* problems, int32_t n, const mc_
         e = cudaMemcpy(b->d_offsets, offs.data(), sizeof(long long) * n, cudaMemcpyHostToDevice);
     }
     if (e == cudaSuccess) {
-        e = cudaMemset(b->d_counters, 0, sizeof(int) * 4);
+        e = cudaMemset(b->d_counters, 0, sizeof(int) * kCounters);
     }
     if (e != cudaSuccess) {
         mc_batch_destroy(b);
@@ -439,15 +482,19 @@ mc_status mc_batch_create(const mc_batch_problem* problems, int32_t n, const mc_
         mc_batch_destroy(b);
         return st;
     }
-    int occ = 0;
-    const BatchStageParams probe = stage_params(b, nullptr, 0, 0, 1, mc::kAdd, 0, 0, b->d_counters);
-    e = launch_stage(b, probe, 1, b->stream, &occ);
-    if (e != cudaSuccess) {
-        mc_batch_destroy(b);
-        return bcuda(e, "occupancy");
+    int occ[2] = {0, 0};
+    for (int part : {mc::kPart2d, mc::kPart1d}) {
+        const BatchStageParams probe = stage_params(b, part, 0, 0, b->d_counters);
+        e = launch_stage(b, probe, part, 1, b->stream, &occ[part]);
+        if (e != cudaSuccess) {
+            mc_batch_destroy(b);
+            return bcuda(e, "occupancy");
+        }
     }
-    b->occupancy = std::max(occ, 1);
+    b->occupancy = std::max(occ[mc::kPart2d], 1);
+    b->occupancy1d = std::max(occ[mc::kPart1d], 1);
     b->grid = b->sms * b->occupancy;
+    b->grid1d = b->sms * b->occupancy1d;
     *out = b;
     return MC_OK;
 }
@@ -463,6 +510,7 @@ mc_status mc_batch_destroy(mc_batch* b) {
     cudaFree(b->buf_b);
     cudaFree(b->d_params);
     cudaFree(b->d_offsets);
+    cudaFree(b->d_stage);
     cudaFree(b->d_blocks);
     cudaFree(b->d_counters);
     cudaFree(b->d_items2d);
@@ -506,55 +554,81 @@ mc_status mc_batch_tune(mc_batch* b, double* pool, void* stream) {
             return st;
         }
     }
+    if (mc_status st = bind_stages(b, pool)) {
+        return st;
+    }
     cudaEvent_t t0, t1;
     MCB_CUDA(cudaEventCreate(&t0), "event");
     MCB_CUDA(cudaEventCreate(&t1), "event");
-    const int grids[4] = {b->sms * b->occupancy, 2 * b->sms * b->occupancy, 4 * b->sms * b->occupancy, -1};
-    const int segs_opts[3] = {1, 2, 4};
-    float best = 1e30f;
-    int best_grid = b->grid, best_dyn = b->dynamic, best_segs = b->segs;
-    for (int so : segs_opts) {
-        if (mc_status st = build_tasks(b, so)) {
-            return st;
+    // time one launch of `part` (stage 0: reads the pool, writes buffer A
+    // only), best of three
+    auto time_part = [&](int part, int grid, int dyn, float* out) -> mc_status {
+        float tmin = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            MCB_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(int) * kCounters, b->stream), "counters");
+            const BatchStageParams bp = stage_params(b, part, 0, dyn, b->d_counters);
+            MCB_CUDA(cudaEventRecord(t0, b->stream), "event");
+            MCB_CUDA(launch_stage(b, bp, part, grid, b->stream, nullptr), "tune launch");
+            MCB_CUDA(cudaEventRecord(t1, b->stream), "event");
+            MCB_CUDA(cudaEventSynchronize(t1), "event");
+            float ms = 0.f;
+            MCB_CUDA(cudaEventElapsedTime(&ms, t0, t1), "event");
+            tmin = std::min(tmin, ms);
         }
-        const int n_items = b->n2d + cdiv(b->ntasks1d, mc::kWarps);
+        *out = tmin;
+        return MC_OK;
+    };
+    // candidate grids: 1, 2 or 4 waves of resident CTAs, or one CTA per work
+    // item (-1: a plain, non-persistent launch, static only)
+    auto sweep = [&](int part, int occ, int n_items, int* best_grid, int* best_dyn, float* best) -> mc_status {
+        const int grids[4] = {b->sms * occ, 2 * b->sms * occ, 4 * b->sms * occ, -1};
         for (int gi = 0; gi < 4; ++gi) {
             for (int dyn = 0; dyn < 2; ++dyn) {
-                // grid -1: one CTA per work item (a plain, non-persistent launch)
-                const int grid = grids[gi] > 0 ? std::min(grids[gi], n_items) : n_items;
                 if (grids[gi] < 0 && dyn) {
                     continue;
                 }
-                float tmin = 1e30f;
-                for (int rep = 0; rep < 3; ++rep) {
-                    MCB_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(int) * 4, b->stream), "counters");
-                    // stage 0 reads the pool and writes buffer A only
-                    const BatchStageParams bp = stage_params(b, pool, 0, 0, 1, plan_for(b->scheme.time_stepper).combo[0],
-                                                             0, dyn, b->d_counters);
-                    MCB_CUDA(cudaEventRecord(t0, b->stream), "event");
-                    MCB_CUDA(launch_stage(b, bp, grid, b->stream, nullptr), "tune launch");
-                    MCB_CUDA(cudaEventRecord(t1, b->stream), "event");
-                    MCB_CUDA(cudaEventSynchronize(t1), "event");
-                    float ms = 0.f;
-                    MCB_CUDA(cudaEventElapsedTime(&ms, t0, t1), "event");
-                    tmin = std::min(tmin, ms);
+                const int grid = grids[gi] > 0 ? std::min(grids[gi], n_items) : n_items;
+                float ms = 0.f;
+                if (mc_status st = time_part(part, grid, dyn, &ms)) {
+                    return st;
                 }
-                if (tmin < best) {
-                    best = tmin;
-                    best_grid = grid;
-                    best_dyn = dyn;
-                    best_segs = so;
+                if (ms < *best) {
+                    *best = ms;
+                    *best_grid = grid;
+                    *best_dyn = dyn;
                 }
             }
         }
+        return MC_OK;
+    };
+    if (b->n2d > 0) {
+        float best = 1e30f;
+        if (mc_status st = sweep(mc::kPart2d, b->occupancy, b->n2d, &b->grid, &b->dynamic, &best)) {
+            return st;
+        }
+    }
+    if (b->ntasks1d > 0) {
+        float best = 1e30f;
+        int best_segs = b->segs;
+        for (int so : {1, 2, 4}) {
+            if (mc_status st = build_tasks(b, so)) {
+                return st;
+            }
+            const float before = best;
+            if (mc_status st = sweep(mc::kPart1d, b->occupancy1d, cdiv(b->ntasks1d, mc::kWarps), &b->grid1d,
+                                     &b->dynamic1d, &best)) {
+                return st;
+            }
+            if (best < before) {
+                best_segs = so;
+            }
+        }
+        b->segs = best_segs;
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
-    MCB_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(int) * 4, b->stream), "counters");
+    MCB_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(int) * kCounters, b->stream), "counters");
     MCB_CUDA(cudaStreamSynchronize(b->stream), "sync");
-    b->grid = best_grid;
-    b->dynamic = best_dyn;
-    b->segs = best_segs;
     return build_tasks(b, b->segs);
 }
 

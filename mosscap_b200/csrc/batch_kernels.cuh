@@ -1,14 +1,16 @@
-// Batched stage kernel: one persistent launch advances one SSPRK stage of
+// Batched stage kernels: persistent launches advance one SSPRK stage of
 // every problem of a batch of independent 1D and 2D problems of uneven size.
 //
-// The work list holds 2D tiles (one CTA each, the tile2d body of the single
-// problem kernel) followed by bundles of kWarps 1D tasks (one warp each, a
-// task being `nseg` consecutive 30-cell segments of one 1D problem, the
-// segment1d body), so the warps of one CTA may serve different small
-// problems. CTAs take work items either statically (item = blockIdx.x +
-// k * gridDim.x) or dynamically from an atomic counter; the autotuner picks.
-// Every problem has its own DeviceBlock: its dt, clock, CFL-minimum cell and
-// status, so each problem advances with its own dt.
+// Two work lists, one kernel each (PART): the 2D tiles (one CTA each, the
+// tile2d body of the single-problem kernel) and bundles of kWarps 1D tasks
+// (one warp each, a task being `nseg` consecutive 30-cell segments of one 1D
+// problem, the segment1d body), so the warps of one CTA may serve different
+// small problems. Keeping the two bodies in separate kernels keeps each
+// kernel's instruction footprint that of one body. CTAs take work items
+// either statically (item = blockIdx.x + k * gridDim.x) or dynamically from
+// an atomic counter; the autotuner picks. Every problem has its own
+// DeviceBlock: its dt, clock, CFL-minimum cell and status, so each problem
+// advances with its own dt.
 #pragma once
 
 #include "stage_kernels.cuh"
@@ -23,45 +25,36 @@ struct BatchTask1d {
 };
 
 struct BatchStageParams {
-    const StageParams* probs;   // per-problem parameters (state pointers unset)
-    const long long* offsets;   // per-problem offset into the state pools
+    // per-problem parameters of this stage (state pointers, combination and
+    // last-stage flag bound), read in place from global memory
+    const StageParams* probs;
     const BatchItem2d* items2d;
     int n2d;
     const BatchTask1d* tasks1d;
     int ntasks1d;
-    int n_items;                // n2d + bundles of kWarps 1D tasks
-    const double* in_base;      // pool of the stage input
-    const double* old_base;     // pool of the step-start state
-    double* out_base;           // pool of the stage output
-    int combo;
-    int last;
+    int n_items;                // work items of this launch: n2d tiles, or bundles of kWarps 1D tasks
     int dynamic;
     int* counter;               // work counter of this launch (dynamic schedule)
 };
 
-template <int REC, class T>
+constexpr int kPart2d = 0;  // the launch over the 2D tiles
+constexpr int kPart1d = 1;  // the launch over the 1D task bundles
+
+template <int REC, class T, int PART>
 __host__ __device__ constexpr size_t batch_smem_bytes() {
-    // a 2D tile of 4 variables or kWarps 1D windows of 3 variables
-    return smem_bytes<2, REC, T>(4) > smem_bytes<1, REC, T>(3) ? smem_bytes<2, REC, T>(4)
-                                                               : smem_bytes<1, REC, T>(3);
+    // a 2D tile of 4 variables, or kWarps 1D windows of 3 variables
+    return PART == kPart2d ? smem_bytes<2, REC, T>(4) : smem_bytes<1, REC, T>(3);
 }
 
-__device__ __forceinline__ void bind_problem(StageParams& sp, const BatchStageParams& bp, int prob) {
-    sp = bp.probs[prob];
-    const long long off = bp.offsets[prob];
-    sp.q_in = bp.in_base + off;
-    sp.q_old = bp.old_base + off;
-    sp.q_out = bp.out_base + off;
-    sp.combo = bp.combo;
-    sp.last = bp.last;
-    sp.reset_min = 0;
-}
+// CTAs per SM of the batched kernels: the per-problem parameters come from
+// global memory rather than the constant bank, so the tile body needs more
+// registers than the single-problem kernel to keep them resident (two CTAs
+// with up to 128 registers measured 7 % faster than three with 80).
+constexpr int kMinBlocksBatch = 2;
 
-template <int REC, int LIM, int RS, class T>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : kMinBlocks2d)
-    batch_stage_kernel(BatchStageParams bp) {
+template <int REC, int LIM, int RS, class T, int PART>
+__global__ void __launch_bounds__(kThreads, kMinBlocksBatch) batch_stage_kernel(BatchStageParams bp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ StageParams sp[kWarps];
     __shared__ double red_d[kWarps];
     __shared__ unsigned red_u[kWarps];
     __shared__ int s_item;
@@ -80,27 +73,22 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : k
         if (item >= bp.n_items) {
             break;
         }
-        if (item < bp.n2d) {
+        if constexpr (PART == kPart2d) {
+            // the problem's parameters, bound to this stage's buffers, are
+            // read in place from global memory
             const BatchItem2d it = bp.items2d[item];
-            if (threadIdx.x == 0) {
-                bind_problem(sp[0], bp, it.prob);
-            }
-            __syncthreads();
-            if (!sp[0].blk->done) {
+            const StageParams& p = bp.probs[it.prob];
+            if (!p.blk->done) {
                 double dtmin = __longlong_as_double((long long)kInfBits);
                 unsigned flags = 0;
-                tile2d<2, REC, LIM, RS, T>(sp[0], it.bx, it.by, 0, smem, dtmin, flags);
-                block_publish(dtmin, flags, sp[0].last != 0, sp[0].blk, red_d, red_u);
+                tile2d<2, REC, LIM, RS, T>(p, it.bx, it.by, 0, smem, dtmin, flags);
+                block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
             }
         } else {
-            const int t = (item - bp.n2d) * kWarps + warp;
+            const int t = item * kWarps + warp;
             if (t < bp.ntasks1d) {
                 const BatchTask1d task = bp.tasks1d[t];
-                if (lane == 0) {
-                    bind_problem(sp[warp], bp, task.prob);
-                }
-                __syncwarp();
-                const StageParams& p = sp[warp];
+                const StageParams& p = bp.probs[task.prob];
                 if (!p.blk->done) {
                     double dtmin = __longlong_as_double((long long)kInfBits);
                     unsigned flags = 0;

@@ -17,10 +17,10 @@ namespace {
 
 using Real = MC_REAL;
 
-template <int REC, int LIM, int RS>
-cudaError_t launch_batch_one(const BatchStageParams& bp, int grid, cudaStream_t s, int* occupancy) {
-    auto k = batch_stage_kernel<REC, LIM, RS, Real>;
-    const size_t sm = batch_smem_bytes<REC, Real>();
+template <int REC, int LIM, int RS, int PART>
+cudaError_t launch_batch_part(const BatchStageParams& bp, int grid, cudaStream_t s, int* occupancy) {
+    auto k = batch_stage_kernel<REC, LIM, RS, Real, PART>;
+    const size_t sm = batch_smem_bytes<REC, Real, PART>();
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) {
         return e;
@@ -32,45 +32,51 @@ cudaError_t launch_batch_one(const BatchStageParams& bp, int grid, cudaStream_t 
     return cudaGetLastError();
 }
 
+template <int REC, int LIM, int RS>
+cudaError_t launch_batch_one(const BatchStageParams& bp, int part, int grid, cudaStream_t s, int* occupancy) {
+    return part == kPart2d ? launch_batch_part<REC, LIM, RS, kPart2d>(bp, grid, s, occupancy)
+                           : launch_batch_part<REC, LIM, RS, kPart1d>(bp, grid, s, occupancy);
+}
+
 template <int REC, int LIM>
-cudaError_t batch_by_solver(const BatchStageParams& bp, int rs, int grid, cudaStream_t s, int* occ) {
+cudaError_t batch_by_solver(const BatchStageParams& bp, int rs, int part, int grid, cudaStream_t s, int* occ) {
     switch (rs) {
         case kRusanov:
-            return launch_batch_one<REC, LIM, kRusanov>(bp, grid, s, occ);
+            return launch_batch_one<REC, LIM, kRusanov>(bp, part, grid, s, occ);
         case kHll:
-            return launch_batch_one<REC, LIM, kHll>(bp, grid, s, occ);
+            return launch_batch_one<REC, LIM, kHll>(bp, part, grid, s, occ);
         default:
-            return launch_batch_one<REC, LIM, kHllc>(bp, grid, s, occ);
+            return launch_batch_one<REC, LIM, kHllc>(bp, part, grid, s, occ);
     }
 }
 
 } // namespace
 
-cudaError_t MC_BATCH_LAUNCH_NAME(const BatchStageParams& bp, int rec, int lim, int rs, int grid, cudaStream_t s,
-                                 int* occupancy) {
+cudaError_t MC_BATCH_LAUNCH_NAME(const BatchStageParams& bp, int rec, int lim, int rs, int part, int grid,
+                                 cudaStream_t s, int* occupancy) {
     switch (rec) {
         case kFog:
-            return batch_by_solver<kFog, kMonotonizedCentral>(bp, rs, grid, s, occupancy);
+            return batch_by_solver<kFog, kMonotonizedCentral>(bp, rs, part, grid, s, occupancy);
         case kMuscl:
             switch (lim) {
                 case kVanLeer:
-                    return batch_by_solver<kMuscl, kVanLeer>(bp, rs, grid, s, occupancy);
+                    return batch_by_solver<kMuscl, kVanLeer>(bp, rs, part, grid, s, occupancy);
                 case kMonotonizedCentral:
-                    return batch_by_solver<kMuscl, kMonotonizedCentral>(bp, rs, grid, s, occupancy);
+                    return batch_by_solver<kMuscl, kMonotonizedCentral>(bp, rs, part, grid, s, occupancy);
                 default:
-                    return batch_by_solver<kMuscl, kMinmod>(bp, rs, grid, s, occupancy);
+                    return batch_by_solver<kMuscl, kMinmod>(bp, rs, part, grid, s, occupancy);
             }
         case kPpm:
             switch (lim) {
                 case kVanLeer:
-                    return batch_by_solver<kPpm, kVanLeer>(bp, rs, grid, s, occupancy);
+                    return batch_by_solver<kPpm, kVanLeer>(bp, rs, part, grid, s, occupancy);
                 case kMonotonizedCentral:
-                    return batch_by_solver<kPpm, kMonotonizedCentral>(bp, rs, grid, s, occupancy);
+                    return batch_by_solver<kPpm, kMonotonizedCentral>(bp, rs, part, grid, s, occupancy);
                 default:
-                    return batch_by_solver<kPpm, kMinmod>(bp, rs, grid, s, occupancy);
+                    return batch_by_solver<kPpm, kMinmod>(bp, rs, part, grid, s, occupancy);
             }
         default:
-            return batch_by_solver<kWeno5z, kMonotonizedCentral>(bp, rs, grid, s, occupancy);
+            return batch_by_solver<kWeno5z, kMonotonizedCentral>(bp, rs, part, grid, s, occupancy);
     }
 }
 
