@@ -46,6 +46,7 @@ typedef enum {
 #define MC_FLAG_NEG_DENSITY 0x2u   /* rho <= 0 */
 #define MC_FLAG_NEG_PRESSURE 0x4u  /* p <= 0 */
 #define MC_FLAG_BAD_DT 0x8u        /* dt <= 0 or not finite */
+#define MC_FLAG_EOS 0x10u          /* a non-ideal EOS update met a state the reference aborts on */
 
 /* Enum values equal the reference's ordinals. */
 typedef enum { /* source/Reconstruct.hpp:10-15 */
@@ -146,6 +147,50 @@ mc_status mc_destroy(mc_ctx* ctx);
  * mc_advance may call it for steps the device has already skipped. Required
  * when any active face is MC_BC_USERFN. fn = NULL removes the hook. */
 mc_status mc_set_user_bc(mc_ctx* ctx, void (*fn)(void* user, double* Q, void* stream), void* user);
+
+/* ---- Non-ideal equations of state --------------------------------------------
+ *
+ * The EOS kinds of the reference (EosType ordinals, source/Eos.hpp:16-21);
+ * the DexRT-coupled kind is out of scope. */
+typedef enum {
+    MC_EOS_IDEAL = 0,
+    MC_EOS_ANALYTIC_LTE_H = 1,   /* source/AnalyticLteH.hpp */
+    MC_EOS_TABULATED_LTE_H = 2   /* source/TabulatedLteH.hpp */
+} mc_eos_type;
+
+/* Table of the tabulated LTE hydrogen EOS (the NetCDF variables the
+ * reference reads, source/TabulatedLteH.hpp:30-58): ionisation fraction y
+ * and log10 T on a grid uniform in log10(eint / rho) (fastest) and
+ * log10(rho); host arrays of n_rho x n_eint_rho values, copied. */
+typedef struct {
+    double log_eint_rho_start, log_eint_rho_step;
+    int32_t n_eint_rho;
+    double log_rho_start, log_rho_step;
+    int32_t n_rho;
+    const double* y_table;
+    const double* log_T_table;
+} mc_eos_table;
+
+/* Selects the EOS, as Eos::init does (source/Eos.cpp:11-86; avg_mass is the
+ * config key eos.avg_mass, include_ionisation_energy
+ * eos.include_ionisation_energy, table the file eos.table_path holds). For a
+ * non-ideal kind the update runs ahead of every stage on the stage's input
+ * state, cells and ghosts (compute_hydro_fluxes, source/Hydro.cpp:326-328):
+ * the analytic kind computes the temperature and ionisation fraction fields
+ * by bisection and leaves the state alone; the tabulated kind interpolates
+ * them and shifts the energy by the ionisation energy of the change of y
+ * since the previous update (the step-start state keeps its energy, as the
+ * reference's Q_old copy does). Results agree with the reference to the
+ * rounding of pow / exp / log10. */
+mc_status mc_set_eos(mc_ctx* ctx, int32_t type, double avg_mass, int32_t include_ionisation_energy,
+                     const mc_eos_table* table);
+/* One EOS update of Q in place, as setup_sim makes before the first step
+ * (source/SetupModules.hpp:253-255). */
+mc_status mc_update_eos(mc_ctx* ctx, double* Q, void* stream);
+/* Copies the fields of the last update, y_space and T_space (zc*yc*xc
+ * doubles each, the layout of one variable of Q), to y and T (device or
+ * host memory; either may be NULL). */
+mc_status mc_get_eos_fields(mc_ctx* ctx, double* y, double* T, void* stream);
 
 /* Registers the gravity source term (setup_gravity,
  * source/SourceTerms/Gravity.cpp:44-70; config keys sources.gravity.x/y/z):

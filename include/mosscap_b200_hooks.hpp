@@ -10,10 +10,11 @@
 //
 // The state stays in Mosscap's own device array (sim.state.Q.data()); the
 // library owns only its two stage buffers. Requirements: a CUDA build of
-// Mosscap in double precision (fp_t = f64), the ideal EOS, no source term
-// other than gravity (whose vector install() must be given, since the
-// registered std::function does not expose it); fill_bcs at setup can stay
-// Mosscap's own or use mc_fill_bcs.
+// Mosscap in double precision (fp_t = f64), the ideal, analytic or tabulated
+// EOS, no source term other than gravity (the gravity vector and a non-ideal
+// EOS's settings must be given to install(), since the registered
+// std::functions do not expose them); fill_bcs at setup can stay Mosscap's
+// own or use mc_fill_bcs.
 #pragma once
 
 #include <memory>
@@ -74,13 +75,35 @@ Context make_context(const Sim& sim) {
     return Context(c, ContextDeleter{});
 }
 
+// The equation of state a Simulation was set up with (Eos::init,
+// source/Eos.cpp:11-86): the eos.type ordinal, eos.avg_mass,
+// eos.include_ionisation_energy and, for the tabulated kind, the table read
+// from eos.table_path. The registered update_eos does not expose them.
+struct EosConfig {
+    int type;
+    double avg_mass;
+    bool include_ionisation_energy;
+    const mc_eos_table* table;
+};
+
 // Replace Simulation::time_step and Simulation::compute_dt. gravity: the
 // sources.gravity.{x,y,z} values of the configuration, required when the
 // Simulation registered the gravity source term (setup_gravity,
-// source/SourceTerms/Gravity.cpp:44-70).
+// source/SourceTerms/Gravity.cpp:44-70). eos: required when the Simulation
+// has an update_eos (a non-ideal EOS); the library then runs the update
+// ahead of every stage and copies y_space / T_space into sim.eos after each
+// step, where Mosscap's output and coupling read them.
 template <class Sim>
-Context install(Sim& sim, const double* gravity = nullptr) {
+Context install(Sim& sim, const double* gravity = nullptr, const EosConfig* eos = nullptr) {
     Context ctx = make_context(sim);
+    const bool non_ideal = bool(sim.update_eos);
+    if (non_ideal) {
+        if (!eos) {
+            throw std::runtime_error("mosscap_b200: a non-ideal EOS needs its EosConfig in install()");
+        }
+        check(mc_set_eos(ctx.get(), eos->type, eos->avg_mass, eos->include_ionisation_energy ? 1 : 0, eos->table),
+              "mc_set_eos");
+    }
     bool has_gravity = false;
     for (const auto& term : sim.compute_source_terms) {
         if (term.name != "gravity") {
@@ -94,8 +117,12 @@ Context install(Sim& sim, const double* gravity = nullptr) {
         }
         check(mc_set_gravity(ctx.get(), 1, gravity[0], gravity[1], gravity[2]), "mc_set_gravity");
     }
-    sim.time_step = [ctx](Sim& s, auto dt) {
+    sim.time_step = [ctx, non_ideal](Sim& s, auto dt) {
         check(mc_time_step(ctx.get(), s.state.Q.data(), double(dt), nullptr), "mc_time_step");
+        if (non_ideal) {
+            check(mc_get_eos_fields(ctx.get(), s.eos.y_space.data(), s.eos.T_space.data(), nullptr),
+                  "mc_get_eos_fields");
+        }
         s.dt = dt;
         s.time += dt;
         s.current_step += 1;

@@ -19,6 +19,8 @@ MC_OK = 0
 STATUS_NAMES = {0: "MC_OK", 1: "MC_ERR_INVALID_ARGUMENT", 2: "MC_ERR_UNSUPPORTED", 3: "MC_ERR_CUDA",
                 4: "MC_ERR_OUT_OF_MEMORY", 5: "MC_ERR_STATE"}
 FLAG_NONFINITE, FLAG_NEG_DENSITY, FLAG_NEG_PRESSURE, FLAG_BAD_DT = 0x1, 0x2, 0x4, 0x8
+FLAG_EOS = 0x10
+EOS = {"ideal": 0, "analyticlteh": 1, "tabulatedlteh": 2}
 
 RECON = {"fog": 0, "muscl": 1, "ppm": 2, "weno5z": 3}
 LIMITER = {"vanleer": 0, "monotonizedcentral": 1, "minmod": 2}
@@ -73,6 +75,17 @@ class McBatchProblem(ctypes.Structure):
 
 
 USER_BC_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
+
+
+class McEosTable(ctypes.Structure):
+    _fields_ = [
+        ("log_eint_rho_start", ctypes.c_double), ("log_eint_rho_step", ctypes.c_double),
+        ("n_eint_rho", ctypes.c_int32),
+        ("log_rho_start", ctypes.c_double), ("log_rho_step", ctypes.c_double),
+        ("n_rho", ctypes.c_int32),
+        ("y_table", ctypes.POINTER(ctypes.c_double)),
+        ("log_T_table", ctypes.POINTER(ctypes.c_double)),
+    ]
 
 
 class McError(RuntimeError):
@@ -136,6 +149,12 @@ def load() -> ctypes.CDLL:
     lib.mc_time_step_noalloc.restype = i32
     lib.mc_set_gravity.argtypes = [vp, i32, d, d, d]
     lib.mc_set_gravity.restype = i32
+    lib.mc_set_eos.argtypes = [vp, i32, d, i32, P(McEosTable)]
+    lib.mc_set_eos.restype = i32
+    lib.mc_update_eos.argtypes = [vp, vp, vp]
+    lib.mc_update_eos.restype = i32
+    lib.mc_get_eos_fields.argtypes = [vp, vp, vp, vp]
+    lib.mc_get_eos_fields.restype = i32
     lib.mc_launch_count.argtypes = [vp]
     lib.mc_launch_count.restype = i64
     lib.mc_adjoint_create.argtypes = [P(McGrid), P(McScheme), i32, P(vp)]

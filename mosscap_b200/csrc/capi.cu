@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "eos.h"
 #include "launch.h"
 #include "mosscap_b200.h"
 
@@ -36,6 +37,17 @@ struct mc_ctx {
     void* user_bc_data = nullptr;
     int gravity = 0;              // mc_set_gravity
     double grav[3] = {0.0, 0.0, 0.0};
+    // non-ideal EOS (mc_set_eos)
+    int eos_type = 0;
+    int eos_ion = 0;
+    double eos_avg_mass = 1.0;
+    double* eos_y = nullptr;      // y_space, T_space (device, plane each)
+    double* eos_T = nullptr;
+    double* eos_ytab = nullptr;   // tabulated: tables (device) and grid
+    double* eos_lTtab = nullptr;
+    double tab_x0 = 0.0, tab_dx = 1.0, tab_y0 = 0.0, tab_dy = 1.0;
+    int tab_nx = 0, tab_ny = 0;
+    double* buf_eos = nullptr;    // tabulated: the first stage's shifted input
     // kernel timing (mc_profile_stages)
     bool profiling = false;
     struct Timed {
@@ -171,6 +183,32 @@ cudaError_t launch_stage_kernel(mc_ctx* c, const StageParams& p, int pass, cudaS
     return f32 ? mc::launch_stage_d3_fp32(p, r, l, rs, pass, s) : mc::launch_stage_d3_fp64(p, r, l, rs, pass, s);
 }
 
+mc::EosLaunch eos_launch(const mc_ctx* c, const double* q_in, double* q_out, bool skip_when_done) {
+    mc::EosLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.type = c->eos_type;
+    L.q_in = q_in;
+    L.q_out = q_out;
+    L.y = c->eos_y;
+    L.T = c->eos_T;
+    L.plane = c->plane;
+    L.nvar = c->nvar;
+    L.gamma = c->scheme.gamma;
+    L.avg_mass = c->eos_avg_mass;
+    L.ionisation_e = c->eos_ion;
+    L.x_start = c->tab_x0;
+    L.x_step = c->tab_dx;
+    L.y_start = c->tab_y0;
+    L.y_step = c->tab_dy;
+    L.nx_tab = c->tab_nx;
+    L.ny_tab = c->tab_ny;
+    L.y_table = c->eos_ytab;
+    L.log_T_table = c->eos_lTtab;
+    L.blk = c->blk;
+    L.skip_when_done = skip_when_done ? 1 : 0;
+    return L;
+}
+
 // Enqueue one SSPRK step on Q. dt_dev (device-driven loop) or dt (host).
 mc_status enqueue_step(mc_ctx* c, double* Q, double dt, const double* dt_dev, bool reset_min, cudaStream_t s) {
     const StagePlan plan = plan_for(c->scheme.time_stepper);
@@ -186,6 +224,20 @@ mc_status enqueue_step(mc_ctx* c, double* Q, double dt, const double* dt_dev, bo
         p.combo = plan.combo[st];
         p.last = st == plan.n - 1;
         p.reset_min = (reset_min && st == 0) ? 1 : 0;
+        if (c->eos_type != mc::kEosIdeal) {
+            // update_eos ahead of the sweep; the tabulated kind shifts the
+            // energy, which for the first stage goes to a copy so that the
+            // step-start state keeps its own
+            double* q_eos = const_cast<double*>(p.q_in);
+            if (c->eos_type == mc::kEosTabulated && p.q_in == Q) {
+                q_eos = c->buf_eos;
+                p.q_in = q_eos;
+            }
+            c->launches += 1;
+            MC_CUDA(mc::launch_eos_update(eos_launch(c, bufs[plan.in[st]], q_eos, dt_dev != nullptr),
+                                          c->grid.num_dim, s),
+                    "EOS update");
+        }
         MC_CUDA(launch_stage(c, p, 0, s), "stage launch");
         if (c->grid.num_dim == 3) {
             p.reset_min = 0;
@@ -347,6 +399,11 @@ mc_status mc_destroy(mc_ctx* c) {
     cudaFree(c->dqxy);
     cudaFree(c->blk);
     cudaFree(c->dt_log);
+    cudaFree(c->eos_y);
+    cudaFree(c->eos_T);
+    cudaFree(c->eos_ytab);
+    cudaFree(c->eos_lTtab);
+    cudaFree(c->buf_eos);
     if (c->blk_host) {
         cudaFreeHost(c->blk_host);
     }
@@ -378,6 +435,90 @@ mc_status mc_set_gravity(mc_ctx* c, int32_t enabled, double gx, double gy, doubl
     c->grav[0] = enabled ? gx : 0.0;
     c->grav[1] = enabled && c->grid.num_dim > 1 ? gy : 0.0;
     c->grav[2] = enabled && c->grid.num_dim > 2 ? gz : 0.0;
+    return MC_OK;
+}
+
+mc_status mc_set_eos(mc_ctx* c, int32_t type, double avg_mass, int32_t include_ionisation_energy,
+                     const mc_eos_table* t) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    if (type < MC_EOS_IDEAL || type > MC_EOS_TABULATED_LTE_H || !(avg_mass > 0.0)) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "unknown EOS type or avg_mass <= 0");
+    }
+    if (type == MC_EOS_TABULATED_LTE_H &&
+        (!t || !t->y_table || !t->log_T_table || t->n_eint_rho < 1 || t->n_rho < 1 ||
+         !(t->log_eint_rho_step > 0.0) || !(t->log_rho_step > 0.0))) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "the tabulated EOS needs a table with positive steps");
+    }
+    c->eos_type = type;
+    c->eos_avg_mass = avg_mass;
+    c->eos_ion = include_ionisation_energy ? 1 : 0;
+    if (type == MC_EOS_IDEAL) {
+        return MC_OK;
+    }
+    const size_t cells = (size_t)c->plane;
+    if (!c->eos_y) {
+        MC_CUDA(cudaMalloc(&c->eos_y, sizeof(double) * cells), "EOS fields");
+        MC_CUDA(cudaMalloc(&c->eos_T, sizeof(double) * cells), "EOS fields");
+    }
+    // Eos::init_* (source/Eos.cpp:40-86): the tabulated kind starts from
+    // y_space = -1, which makes its first energy shift zero
+    std::vector<double> init(cells, type == MC_EOS_TABULATED_LTE_H ? -1.0 : 0.0);
+    MC_CUDA(cudaMemcpy(c->eos_y, init.data(), sizeof(double) * cells, cudaMemcpyHostToDevice), "EOS fields");
+    MC_CUDA(cudaMemset(c->eos_T, 0, sizeof(double) * cells), "EOS fields");
+    if (type == MC_EOS_TABULATED_LTE_H) {
+        const size_t n = (size_t)t->n_rho * (size_t)t->n_eint_rho;
+        cudaFree(c->eos_ytab);
+        cudaFree(c->eos_lTtab);
+        c->eos_ytab = c->eos_lTtab = nullptr;
+        MC_CUDA(cudaMalloc(&c->eos_ytab, sizeof(double) * n), "EOS table");
+        MC_CUDA(cudaMalloc(&c->eos_lTtab, sizeof(double) * n), "EOS table");
+        MC_CUDA(cudaMemcpy(c->eos_ytab, t->y_table, sizeof(double) * n, cudaMemcpyHostToDevice), "EOS table");
+        MC_CUDA(cudaMemcpy(c->eos_lTtab, t->log_T_table, sizeof(double) * n, cudaMemcpyHostToDevice), "EOS table");
+        c->tab_x0 = t->log_eint_rho_start;
+        c->tab_dx = t->log_eint_rho_step;
+        c->tab_nx = t->n_eint_rho;
+        c->tab_y0 = t->log_rho_start;
+        c->tab_dy = t->log_rho_step;
+        c->tab_ny = t->n_rho;
+        if (!c->buf_eos) {
+            MC_CUDA(cudaMalloc(&c->buf_eos, c->state_bytes), "EOS stage buffer");
+        }
+    }
+    return MC_OK;
+}
+
+mc_status mc_update_eos(mc_ctx* c, double* Q, void* stream) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    if (!Q) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null Q");
+    }
+    if (c->eos_type == MC_EOS_IDEAL) {
+        return MC_OK;
+    }
+    c->launches += 1;
+    MC_CUDA(mc::launch_eos_update(eos_launch(c, Q, Q, false), c->grid.num_dim, (cudaStream_t)stream), "EOS update");
+    return MC_OK;
+}
+
+mc_status mc_get_eos_fields(mc_ctx* c, double* y, double* T, void* stream) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    if (c->eos_type == MC_EOS_IDEAL || !c->eos_y) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "no non-ideal EOS selected");
+    }
+    const size_t bytes = sizeof(double) * (size_t)c->plane;
+    const cudaStream_t s = (cudaStream_t)stream;
+    if (y) {
+        MC_CUDA(cudaMemcpyAsync(y, c->eos_y, bytes, cudaMemcpyDefault, s), "EOS fields");
+    }
+    if (T) {
+        MC_CUDA(cudaMemcpyAsync(T, c->eos_T, bytes, cudaMemcpyDefault, s), "EOS fields");
+    }
     return MC_OK;
 }
 

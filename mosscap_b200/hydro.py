@@ -71,6 +71,18 @@ class HydroSim:
         if p.gravity is not None:
             gx, gy, gz = (float(x) for x in p.gravity)
             capi.check(self.lib.mc_set_gravity(h, 1, gx, gy, gz), "mc_set_gravity")
+        if p.eos != "ideal":
+            tab = None
+            if p.eos_table is not None:
+                xs, xd, ys, yd, yt, lt = p.eos_table
+                self._eos_y = np.ascontiguousarray(yt, dtype=np.float64)
+                self._eos_t = np.ascontiguousarray(lt, dtype=np.float64)
+                dp = ctypes.POINTER(ctypes.c_double)
+                tab = capi.McEosTable(xs, xd, self._eos_y.shape[1], ys, yd, self._eos_y.shape[0],
+                                      self._eos_y.ctypes.data_as(dp), self._eos_t.ctypes.data_as(dp))
+            with torch.cuda.device(self.device):
+                capi.check(self.lib.mc_set_eos(h, capi.EOS[p.eos], float(p.eos_avg_mass), int(p.eos_ionisation),
+                                               ctypes.byref(tab) if tab is not None else None), "mc_set_eos")
         q = Q if Q is not None else p.Q
         if q is None:
             raise ValueError("no initial state")
@@ -130,6 +142,22 @@ class HydroSim:
         v = ctypes.c_double()
         capi.check(self.lib.mc_last_cfl_min(self.ctx, ctypes.byref(v), self._stream()), "mc_last_cfl_min")
         return v.value
+
+    def update_eos(self) -> None:
+        """One EOS update of Q (Simulation::update_eos, as setup_sim calls it
+        before the first step, source/SetupModules.hpp:253-255)."""
+        capi.check(self.lib.mc_update_eos(self.ctx, self._qptr(), self._stream()), "mc_update_eos")
+
+    def eos_fields(self):
+        """The ionisation fraction and temperature fields of the last EOS
+        update (y_space, T_space), each [zc, yc, xc]."""
+        shape = tuple(self.Q.shape[1:])
+        y = torch.empty(shape, dtype=torch.float64, device=self.device)
+        T = torch.empty(shape, dtype=torch.float64, device=self.device)
+        capi.check(self.lib.mc_get_eos_fields(self.ctx, ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(T.data_ptr()),
+                                              self._stream()), "mc_get_eos_fields")
+        torch.cuda.synchronize(self.device)
+        return y.cpu().numpy(), T.cpu().numpy()
 
     def status(self) -> int:
         f = ctypes.c_uint32()

@@ -43,6 +43,15 @@ class Problem:
     # acceleration of the gravity source term (sources.gravity.x/y/z of the
     # reference's configuration); None: no source term
     gravity: Optional[Tuple[float, float, float]] = None
+    # equation of state (eos.type of the reference's configuration): "ideal",
+    # "analyticlteh" or "tabulatedlteh"; eos.avg_mass,
+    # eos.include_ionisation_energy and, for the tabulated kind, the table
+    # (log_eint_rho_start, log_eint_rho_step, log_rho_start, log_rho_step,
+    # y_table [n_rho, n_eint_rho], log_T_table [n_rho, n_eint_rho])
+    eos: str = "ideal"
+    eos_avg_mass: float = 1.0
+    eos_ionisation: bool = False
+    eos_table: Optional[tuple] = field(default=None, repr=False)
     Q: Optional[np.ndarray] = field(default=None, repr=False)
 
     @property
@@ -276,3 +285,102 @@ def random_state(num_dim: int, nx: int, ny: int = 1, nz: int = 1, ng: int = 3,
     for t in range(num_tracers):
         w[2 + num_dim + t] = 0.5 + 0.4 * np.tanh(smooth() + jumpy())
     return prim_to_cons(num_dim, gamma, w)
+
+
+# ---------------------------------------------------------------------------
+# Partially ionised hydrogen in local thermodynamic equilibrium (SI units), for
+# the non-ideal EOS kinds (source/AnalyticLteH.hpp, source/TabulatedLteH.hpp)
+# ---------------------------------------------------------------------------
+H_MASS = 1.6737830080950003e-27  # [kg]
+K_B = 1.380649e-23               # [J / K]
+CHI_H = 2.178710282685096e-18    # [J]
+
+
+def saha_y(nhtot, temp):
+    """Ionisation fraction of hydrogen from the Saha equation (the
+    reference's y_from_nhtot, source/AnalyticLteH.hpp:10-20)."""
+    X = 2.4146830395719654e+21 * np.power(temp, 1.5) * np.exp(-157763.42386247337 / temp)
+    return 0.5 * (-X + np.sqrt(X * X + 4 * nhtot * X)) / nhtot
+
+
+def lte_internal_energy(rho, temp, gamma, avg_mass=1.0, ionisation=False):
+    """Internal energy density [J / m^3] of LTE hydrogen at (rho, T)."""
+    y = saha_y(rho / (H_MASS * avg_mass), temp)
+    e = rho * (K_B / H_MASS) / avg_mass * (1.0 + y) * temp / (gamma - 1.0)
+    if ionisation:
+        e = e + y * rho * (CHI_H / H_MASS) / avg_mass
+    return e
+
+
+def lte_h_table(n_eint_rho: int = 96, n_rho: int = 48, gamma: float = 5.0 / 3.0,
+                log_rho_range=(-10.0, -5.0), log_t_range=(3.4, 4.6)):
+    """A tabulated LTE hydrogen EOS in the layout the reference reads
+    (source/TabulatedLteH.hpp:30-58): y and log10 T on a grid uniform in
+    log10(eint / rho) and log10(rho), eint including the ionisation energy.
+    Each entry solves eint / rho = (k_B / m_H) (1 + y) T / (gamma - 1) +
+    (chi_H / m_H) y with y from Saha, by bisection in log T."""
+    log_rho = log_rho_range[0] + (log_rho_range[1] - log_rho_range[0]) * np.arange(n_rho) / (n_rho - 1)
+    t_lo, t_hi = 10.0 ** log_t_range[0], 10.0 ** log_t_range[1]
+    e_lo = lte_internal_energy(10.0 ** log_rho[-1], t_lo, gamma, ionisation=True) / 10.0 ** log_rho[-1]
+    e_hi = lte_internal_energy(10.0 ** log_rho[0], t_hi, gamma, ionisation=True) / 10.0 ** log_rho[0]
+    lx0, lx1 = np.log10(e_lo), np.log10(e_hi)
+    log_e = lx0 + (lx1 - lx0) * np.arange(n_eint_rho) / (n_eint_rho - 1)
+    R = 10.0 ** log_rho[:, None] * np.ones((1, n_eint_rho))
+    target = 10.0 ** log_e[None, :] * np.ones((n_rho, 1))
+    a = np.full(R.shape, np.log10(t_lo) - 1.0)
+    b = np.full(R.shape, np.log10(t_hi) + 1.0)
+    for _ in range(200):
+        m = 0.5 * (a + b)
+        f = lte_internal_energy(R, 10.0 ** m, gamma, ionisation=True) / R - target
+        a = np.where(f < 0.0, m, a)
+        b = np.where(f < 0.0, b, m)
+    logt = 0.5 * (a + b)
+    y = saha_y(R / H_MASS, 10.0 ** logt)
+    return (float(lx0), float((lx1 - lx0) / (n_eint_rho - 1)), float(log_rho[0]),
+            float((log_rho[-1] - log_rho[0]) / (n_rho - 1)), y, logt)
+
+
+def lte_hydrogen(num_dim: int, n: int, seed: int = 0, eos: str = "analyticlteh", gamma: float = 5.0 / 3.0,
+                 avg_mass: float = 1.0, ionisation: bool = False, ng: int = 3, table=None) -> Problem:
+    """Partially ionised hydrogen in LTE: smooth seeded fields of density
+    (1e-9 .. 1e-6 kg / m^3), temperature (5e3 .. 2e4 K) and velocity (up to
+    5 km / s) on a periodic box of n cells per axis of 10 km; the energy
+    includes the ionisation energy when the EOS does (ionisation for the
+    analytic kind, always for the tabulated kind). MUSCL (MC) + HLLC, SSPRK3."""
+    rng = np.random.default_rng(seed)
+    dx = 1.0e4
+    shape = tuple([n + 2 * ng] * num_dim)
+
+    def smooth_field():
+        c = (np.arange(n + 2 * ng) - ng + 0.5) / n
+        grids = np.meshgrid(*([c] * num_dim), indexing="ij")
+        f = np.zeros(shape)
+        for _ in range(3):
+            k = rng.integers(1, 4, size=num_dim)
+            ph = rng.uniform(0, 2 * np.pi, size=num_dim)
+            term = np.ones(shape)
+            for a in range(num_dim):
+                term = term * np.sin(2 * np.pi * k[a] * grids[a] + ph[a])
+            f = f + rng.uniform(0.3, 1.0) * term
+        return f / (np.abs(f).max() + 1e-300)
+
+    rho = 10.0 ** (-7.5 + 1.5 * smooth_field())
+    temp = 10.0 ** (4.0 + 0.3 * smooth_field())
+    vel = [5.0e3 * smooth_field() for _ in range(num_dim)]
+    with_ion = ionisation or eos == "tabulatedlteh"
+    eint = lte_internal_energy(rho, temp, gamma, avg_mass, with_ion)
+    ekin = 0.5 * rho * sum(v * v for v in vel)
+    q = np.empty((2 + num_dim,) + shape)
+    q[0] = rho
+    for a in range(num_dim):
+        q[1 + a] = rho * vel[a]
+    q[1 + num_dim] = eint + ekin
+    # [var][k][j][i] with the active axes last
+    q = q.reshape((2 + num_dim,) + (1,) * (3 - num_dim) + shape)
+    if eos == "tabulatedlteh" and table is None:
+        table = lte_h_table(gamma=gamma)
+    return Problem(f"lte_h_{num_dim}d", num_dim, n, n if num_dim > 1 else 1, n if num_dim > 2 else 1, ng=ng, dx=dx,
+                   bc=("periodic",) * 6, reconstruction="muscl", slope_limiter="monotonizedcentral",
+                   riemann_solver="hllc", time_stepper="ssprk3", gamma=gamma, max_cfl=0.4, max_time=1e30,
+                   output_delta=1e30, eos=eos, eos_avg_mass=avg_mass, eos_ionisation=ionisation, eos_table=table,
+                   Q=q)

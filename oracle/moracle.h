@@ -70,6 +70,33 @@ void moracle_set_num_threads(int n);
  * enabled = 0 leaves the simulation without source terms. */
 void moracle_set_gravity(void* sim, int enabled, double gx, double gy, double gz);
 
+/* Table of the tabulated LTE hydrogen EOS (source/TabulatedLteH.hpp:10-27):
+ * y and log10 T on a grid uniform in log10(eint / rho) (x, fastest) and
+ * log10(rho) (y); arrays [n_rho][n_eint_rho]. */
+typedef struct {
+    double log_eint_rho_start, log_eint_rho_step;
+    int32_t n_eint_rho;
+    double log_rho_start, log_rho_step;
+    int32_t n_rho;
+    const double* y_table;
+    const double* log_T_table;
+} moracle_eos_table;
+/* Selects the EOS (EosType ordinals, source/Eos.hpp:16-21): 0 ideal, 1
+ * analytic LTE hydrogen (include_ionisation_energy as the config key), 2
+ * tabulated LTE hydrogen (table copied). avg_mass is eos.avg_mass. Sets
+ * Simulation::update_eos as Eos::init does (source/Eos.cpp:40-86), which
+ * compute_hydro_fluxes runs ahead of every stage. Returns 0, or -1 for an
+ * unknown type or a missing table. */
+int moracle_set_eos(void* sim, int type, double avg_mass, int include_ionisation_energy,
+                    const moracle_eos_table* table);
+/* One update_eos call, as setup_sim makes before the first step
+ * (source/SetupModules.hpp:253-255). */
+void moracle_update_eos(void* sim);
+/* The EOS fields y_space and T_space, zc * yc * xc values each. */
+void moracle_get_eos_fields(void* sim, double* y, double* T);
+/* Number of conditions on which the reference would have aborted. */
+long long moracle_abort_count(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -38,6 +38,12 @@ typedef struct {
     long long step;
     int gravity;
     double grav[3];
+    /* non-ideal EOS (moracle_set_eos) */
+    int eos_type, eos_ion;
+    double avg_mass;
+    double *y_space, *T_space;
+    moracle_eos_table tab;
+    double *ytab, *lTtab;
 } osim;
 
 /* std::min / std::max semantics (first argument wins ties and NaN compares). */
@@ -396,8 +402,170 @@ static void compute_flux(osim* s, int axis) {
     }
 }
 
-/* compute_hydro_fluxes, source/Hydro.cpp:325-343 */
+/* ---- Non-ideal EOS updates (Simulation::update_eos) ----------------------- */
+
+static const double H_MASS = 1.6737830080950003e-27; /* [kg] */
+static const double K_B = 1.380649e-23;              /* [J / K] */
+static const double CHI_H = 2.178710282685096e-18;    /* [J] */
+
+/* Conditions on which the reference aborts (moracle_abort_count). */
+static long long g_port_aborts = 0;
+
+/* saha_rhs_H, source/AnalyticLteH.hpp:10-14 */
+static double saha_rhs_H(double temp) {
+    return 2.4146830395719654e+21 * pow(temp, 1.5) * exp(-157763.42386247337 / temp);
+}
+
+/* y_from_nhtot, source/AnalyticLteH.hpp:16-20 */
+static double y_from_nhtot(double nhtot, double temp) {
+    const double X = saha_rhs_H(temp);
+    return 0.5 * (-X + sqrt(sq(X) + 4 * nhtot * X)) / nhtot;
+}
+
+/* Kinetic energy and internal energy of cell id (both EOS updates). */
+static void cell_energies(const osim* s, long long id, long long plane, double* rho, double* e_kin, double* eint) {
+    double mom2_sum = sq(s->Q[id + plane]);
+    if (s->ndim > 1) {
+        mom2_sum += sq(s->Q[id + 2 * plane]);
+    }
+    if (s->ndim > 2) {
+        mom2_sum += sq(s->Q[id + 3 * plane]);
+    }
+    *rho = s->Q[id];
+    *e_kin = 0.5 * mom2_sum / *rho;
+    *eint = s->Q[id + (1 + s->ndim) * plane] - *e_kin;
+}
+
+/* AnalyticLteH::update_eos, source/AnalyticLteH.hpp:49-120: temperature and
+ * ionisation fraction by bisection, every cell including ghosts. */
+static void eos_analytic(osim* s) {
+    const long long plane = (long long)s->zc * s->yc * s->xc;
+    const double gamma = s->c.gamma;
+    const int ionisation_e = s->eos_ion;
+    const double inv_avg_mass = 1.0 / s->avg_mass;
+    long long aborts = 0;
+#pragma omp parallel for schedule(static) reduction(+ : aborts)
+    for (long long id = 0; id < plane; ++id) {
+        double rho, e_kin, eint;
+        cell_energies(s, id, plane, &rho, &e_kin, &eint);
+        const double e_to_T = (gamma - 1.0) / (rho * (K_B / H_MASS) * inv_avg_mass);
+#define TEMP_FROM_Y(yy) (e_to_T / (1.0 + (yy)) * (eint - ionisation_e * (yy) * rho * (CHI_H / H_MASS) * inv_avg_mass))
+        const double rho_to_nhtot = (1.0 / H_MASS) * inv_avg_mass;
+        const double min_temperature = 100.0;
+        const double t1 = TEMP_FROM_Y(1.0);
+        const double tb0 = smax(t1, min_temperature);
+        const double tb1 = TEMP_FROM_Y(0.0);
+        if (tb0 > tb1) {
+            aborts += 1;
+        }
+        double temp_step = tb1 - tb0;
+        double temp = tb0;
+        double y = 0.0, test_temp, temp_err;
+        for (int iter = 0; iter < 100; ++iter) {
+            temp_step *= 0.5;
+            test_temp = temp + temp_step;
+            y = y_from_nhtot(rho * rho_to_nhtot, test_temp);
+            temp_err = test_temp - TEMP_FROM_Y(y);
+            if (temp_err <= 0.0) {
+                temp = test_temp;
+            }
+            const double temp_err_bound = 1e-1;
+            if (fabs(temp_step) < temp_err_bound || fabs(temp_err) < temp_err_bound) {
+                break;
+            }
+        }
+#undef TEMP_FROM_Y
+        s->y_space[id] = y;
+        s->T_space[id] = temp;
+    }
+    g_port_aborts += aborts;
+}
+
+/* TabulatedLteH::sample, source/TabulatedLteH.hpp:60-117 */
+static void tab_sample(const osim* s, double log_eint_rho, double log_rho, double* out_y, double* out_log_T) {
+    const moracle_eos_table* t = &s->tab;
+    const double frac_eint_rho = (log_eint_rho - t->log_eint_rho_start) / t->log_eint_rho_step;
+    int ix = (int)floor(frac_eint_rho);
+    int ixp;
+    double tx, txp;
+    const int max_x = t->n_eint_rho - 1;
+    const int max_y = t->n_rho - 1;
+    if (frac_eint_rho < 0.0 || frac_eint_rho >= max_x) {
+        ix = ix < 0 ? 0 : ix;
+        ix = max_x < ix ? max_x : ix;
+        ixp = ix;
+        tx = 1.0;
+        txp = 0.0;
+    } else {
+        ixp = ix + 1;
+        txp = frac_eint_rho - ix;
+        tx = 1.0 - txp;
+    }
+    const double frac_rho = (log_rho - t->log_rho_start) / t->log_rho_step;
+    int iy = (int)floor(frac_rho);
+    int iyp;
+    double ty, typ;
+    if (frac_rho < 0.0 || frac_rho >= max_y) {
+        iy = iy < 0 ? 0 : iy;
+        iy = max_y < iy ? max_y : iy;
+        iyp = iy;
+        ty = 1.0;
+        typ = 0.0;
+    } else {
+        iyp = iy + 1;
+        typ = frac_rho - iy;
+        ty = 1.0 - typ;
+    }
+    const int nx = t->n_eint_rho;
+    const double* Y = s->ytab;
+    const double* L = s->lTtab;
+    *out_y = (ty * (tx * Y[iy * nx + ix] + txp * Y[iy * nx + ixp]) +
+              typ * (tx * Y[iyp * nx + ix] + txp * Y[iyp * nx + ixp]));
+    *out_log_T = (ty * (tx * L[iy * nx + ix] + txp * L[iy * nx + ixp]) +
+                  typ * (tx * L[iyp * nx + ix] + txp * L[iyp * nx + ixp]));
+}
+
+/* TabulatedLteH::update_eos, source/TabulatedLteH.hpp:119-163: y and T from
+ * the table, and the internal energy shifted by the ionisation energy of the
+ * change of y since the previous call, every cell including ghosts. */
+static void eos_tabulated(osim* s) {
+    const long long plane = (long long)s->zc * s->yc * s->xc;
+    long long aborts = 0;
+#pragma omp parallel for schedule(static) reduction(+ : aborts)
+    for (long long id = 0; id < plane; ++id) {
+        double rho, e_kin, eint;
+        cell_energies(s, id, plane, &rho, &e_kin, &eint);
+        const double log_rho = log10(rho);
+        const double log_eint_rho = log10(eint) - log_rho;
+        if (eint < 0.0 || log_eint_rho != log_eint_rho || log_rho != log_rho) {
+            /* the reference aborts here (TabulatedLteH.hpp:142-144); the
+             * restatement counts it and leaves the cell, whose NaN table
+             * coordinates would index out of range */
+            aborts += 1;
+            continue;
+        }
+        double sy, slT;
+        tab_sample(s, log_eint_rho, log_rho, &sy, &slT);
+        const double prev_y = s->y_space[id];
+        s->y_space[id] = sy;
+        const double delta_eint = (prev_y < 0.0) ? 0.0 : rho * (CHI_H / H_MASS) * (sy - prev_y);
+        s->T_space[id] = pow(10.0, slT);
+        s->Q[id + (1 + s->ndim) * plane] += delta_eint;
+    }
+    g_port_aborts += aborts;
+}
+
+static void update_eos(osim* s) {
+    if (s->eos_type == 1) {
+        eos_analytic(s);
+    } else if (s->eos_type == 2) {
+        eos_tabulated(s);
+    }
+}
+
+/* compute_hydro_fluxes, source/Hydro.cpp:325-343 (update_eos first) */
 static void compute_hydro_fluxes(osim* s) {
+    update_eos(s);
     global_cons_to_prim(s);
     for (int a = 0; a < s->ndim; ++a) {
         compute_recon(s, a);
@@ -685,6 +853,10 @@ void moracle_destroy(void* p) {
     free(s->F[1]);
     free(s->F[2]);
     free(s->Qold);
+    free(s->y_space);
+    free(s->T_space);
+    free(s->ytab);
+    free(s->lTtab);
     free(s);
 }
 
@@ -746,6 +918,62 @@ void moracle_set_gravity(void* p, int enabled, double gx, double gy, double gz) 
     s->grav[0] = gx;
     s->grav[1] = gy;
     s->grav[2] = gz;
+}
+
+int moracle_set_eos(void* p, int type, double avg_mass, int include_ionisation_energy,
+                    const moracle_eos_table* t) {
+    osim* s = (osim*)p;
+    const long long plane = (long long)s->zc * s->yc * s->xc;
+    s->avg_mass = avg_mass;
+    s->eos_ion = include_ionisation_energy != 0;
+    if (type == 0) {
+        s->eos_type = 0;
+        return 0;
+    }
+    if (type != 1 && !(type == 2 && t && t->y_table && t->log_T_table)) {
+        return -1;
+    }
+    if (!s->y_space) {
+        s->y_space = (double*)calloc((size_t)plane, sizeof(double));
+        s->T_space = (double*)calloc((size_t)plane, sizeof(double));
+    }
+    for (long long id = 0; id < plane; ++id) {
+        s->y_space[id] = 0.0;
+        s->T_space[id] = 0.0;
+    }
+    s->eos_type = type;
+    if (type == 2) {
+        /* Eos::init_tabulated_lte_h sets y_space = -1 (source/Eos.cpp:75) */
+        const size_t n = (size_t)t->n_rho * (size_t)t->n_eint_rho;
+        free(s->ytab);
+        free(s->lTtab);
+        s->ytab = (double*)malloc(n * sizeof(double));
+        s->lTtab = (double*)malloc(n * sizeof(double));
+        memcpy(s->ytab, t->y_table, n * sizeof(double));
+        memcpy(s->lTtab, t->log_T_table, n * sizeof(double));
+        s->tab = *t;
+        for (long long id = 0; id < plane; ++id) {
+            s->y_space[id] = -1.0;
+        }
+    }
+    return 0;
+}
+
+void moracle_update_eos(void* p) {
+    update_eos((osim*)p);
+}
+
+void moracle_get_eos_fields(void* p, double* y, double* T) {
+    osim* s = (osim*)p;
+    const long long plane = (long long)s->zc * s->yc * s->xc;
+    for (long long id = 0; id < plane; ++id) {
+        y[id] = s->y_space ? s->y_space[id] : 0.0;
+        T[id] = s->T_space ? s->T_space[id] : 0.0;
+    }
+}
+
+long long moracle_abort_count(void) {
+    return g_port_aborts;
 }
 
 void moracle_set_num_threads(int n) {

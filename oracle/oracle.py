@@ -58,6 +58,21 @@ class _Config(ctypes.Structure):
     ]
 
 
+class EosTable(ctypes.Structure):
+    """moracle_eos_table: the tabulated LTE hydrogen EOS grid and tables."""
+    _fields_ = [
+        ("log_eint_rho_start", ctypes.c_double), ("log_eint_rho_step", ctypes.c_double),
+        ("n_eint_rho", ctypes.c_int32),
+        ("log_rho_start", ctypes.c_double), ("log_rho_step", ctypes.c_double),
+        ("n_rho", ctypes.c_int32),
+        ("y_table", ctypes.POINTER(ctypes.c_double)),
+        ("log_T_table", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+EOS_TYPE = {"ideal": 0, "analyticlteh": 1, "tabulatedlteh": 2}
+
+
 def build(kind: str = "all") -> None:
     """Build the oracle libraries with ``oracle/Makefile`` (``make port|ref``)."""
     targets = ["port", "ref"] if kind == "all" else [kind]
@@ -96,6 +111,11 @@ def load(kind: str) -> ctypes.CDLL:
     lib.moracle_set_clock.argtypes = [vp, d, d]
     lib.moracle_set_num_threads.argtypes = [ctypes.c_int]
     lib.moracle_set_gravity.argtypes = [vp, ctypes.c_int, d, d, d]
+    lib.moracle_set_eos.argtypes = [vp, ctypes.c_int, d, ctypes.c_int, ctypes.POINTER(EosTable)]
+    lib.moracle_set_eos.restype = ctypes.c_int
+    lib.moracle_update_eos.argtypes = [vp]
+    lib.moracle_get_eos_fields.argtypes = [vp, dptr, dptr]
+    lib.moracle_abort_count.restype = ctypes.c_longlong
     _LIBS[kind] = lib
     return lib
 
@@ -224,6 +244,37 @@ class OracleSim:
 
     def set_clock(self, time: float, prev_output_time: float) -> None:
         self.lib.moracle_set_clock(self.h, time, prev_output_time)
+
+    def set_eos(self, kind: str, avg_mass: float = 1.0, include_ionisation_energy: bool = False,
+                table=None) -> None:
+        """Select the EOS: "ideal", "analyticlteh" or "tabulatedlteh"; table =
+        (log_eint_rho_start, log_eint_rho_step, log_rho_start, log_rho_step,
+        y_table [n_rho, n_eint_rho], log_T_table [n_rho, n_eint_rho])."""
+        tab = None
+        if table is not None:
+            xs, xd, ys, yd, yt, lt = table
+            self._eos_y = np.ascontiguousarray(yt, dtype=np.float64)
+            self._eos_t = np.ascontiguousarray(lt, dtype=np.float64)
+            tab = EosTable(xs, xd, self._eos_y.shape[1], ys, yd, self._eos_y.shape[0], self._ptr(self._eos_y),
+                           self._ptr(self._eos_t))
+        r = self.lib.moracle_set_eos(self.h, EOS_TYPE[kind], float(avg_mass), int(include_ionisation_energy),
+                                     ctypes.byref(tab) if tab is not None else None)
+        if r != 0:
+            raise ValueError("oracle rejected the EOS")
+
+    def update_eos(self) -> None:
+        self.lib.moracle_update_eos(self.h)
+
+    def eos_fields(self):
+        """(y, T), each [zc, yc, xc]."""
+        shape = self.cfg.shape[1:]
+        y = np.empty(shape, dtype=np.float64)
+        T = np.empty(shape, dtype=np.float64)
+        self.lib.moracle_get_eos_fields(self.h, self._ptr(y), self._ptr(T))
+        return y, T
+
+    def abort_count(self) -> int:
+        return int(self.lib.moracle_abort_count())
 
     def set_gravity(self, g) -> None:
         """Register the gravity source term with acceleration g = (gx, gy, gz);

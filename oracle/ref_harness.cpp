@@ -14,6 +14,8 @@
 #include "Boundaries.hpp"
 #include "SourceTerms.hpp"
 #include "SourceTerms/Gravity.hpp"
+#include "AnalyticLteH.hpp"
+#include "TabulatedLteH.hpp"
 #include "yaml-cpp/yaml.h"
 
 #include <limits>
@@ -214,6 +216,81 @@ void moracle_set_gravity(void* p, int enabled, double gx, double gy, double gz) 
     g.child("y").set(gy);
     g.child("z").set(gz);
     Mosscap::setup_gravity(sim, cfg);
+}
+
+int moracle_set_eos(void* p, int type, double avg_mass, int include_ionisation_energy,
+                    const moracle_eos_table* t) {
+    using namespace Mosscap;
+    Simulation& sim = S(p);
+    Eos& eos = sim.eos;
+    const auto& sz = sim.state.sz;
+    eos.avg_mass = avg_mass;
+    if (type == int(EosType::Ideal)) {
+        eos.is_constant = true;
+        sim.update_eos = nullptr;
+        return 0;
+    }
+    // Eos::init_analytic_lte_h / init_tabulated_lte_h (source/Eos.cpp:40-86),
+    // with the table set in code instead of read from NetCDF
+    eos.is_constant = false;
+    eos.y_space = Fp3d("y_space", sz.zc, sz.yc, sz.xc);
+    eos.T_space = Fp3d("T_space", sz.zc, sz.yc, sz.xc);
+    eos.y_space = 0.0;
+    eos.T_space = 0.0;
+    if (type == int(EosType::AnalyticLteH)) {
+        AnalyticLteH lte;
+        lte.init(include_ionisation_energy != 0);
+        sim.update_eos = [lte](const Simulation& s) {
+            if (s.num_dim == 1) {
+                lte.update_eos<1>(s);
+            } else if (s.num_dim == 2) {
+                lte.update_eos<2>(s);
+            } else {
+                lte.update_eos<3>(s);
+            }
+        };
+        return 0;
+    }
+    if (type == int(EosType::TabulatedLteH) && t && t->y_table && t->log_T_table) {
+        TabulatedLteH lte;
+        lte.eint_rho_grid = TabulatedLteH::LogSpace{t->log_eint_rho_start, t->log_eint_rho_step, t->n_eint_rho};
+        lte.rho_grid = TabulatedLteH::LogSpace{t->log_rho_start, t->log_rho_step, t->n_rho};
+        lte.y_table = Fp2d("y_table", t->n_rho, t->n_eint_rho);
+        lte.log_T_table = Fp2d("log_T_table", t->n_rho, t->n_eint_rho);
+        const size_t n = size_t(t->n_rho) * size_t(t->n_eint_rho);
+        std::memcpy(lte.y_table.data(), t->y_table, sizeof(double) * n);
+        std::memcpy(lte.log_T_table.data(), t->log_T_table, sizeof(double) * n);
+        eos.y_space = -1.0;
+        sim.update_eos = [lte](const Simulation& s) {
+            if (s.num_dim == 1) {
+                lte.update_eos<1>(s);
+            } else if (s.num_dim == 2) {
+                lte.update_eos<2>(s);
+            } else {
+                lte.update_eos<3>(s);
+            }
+        };
+        return 0;
+    }
+    return -1;
+}
+
+void moracle_update_eos(void* p) {
+    auto& sim = S(p);
+    if (sim.update_eos) {
+        sim.update_eos(sim);
+    }
+}
+
+void moracle_get_eos_fields(void* p, double* y, double* T) {
+    auto& eos = S(p).eos;
+    const size_t n = eos.y_space.size();
+    std::memcpy(y, eos.y_space.data(), sizeof(double) * n);
+    std::memcpy(T, eos.T_space.data(), sizeof(double) * n);
+}
+
+long long moracle_abort_count(void) {
+    return Kokkos::abort_count().load();
 }
 
 void moracle_set_num_threads(int n) {

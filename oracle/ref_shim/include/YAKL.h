@@ -19,6 +19,8 @@
 //    reduction identity (the largest finite value).
 #pragma once
 
+#include <atomic>
+
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -34,6 +36,7 @@
 #define KOKKOS_FORCEINLINE_FUNCTION inline
 #define KOKKOS_FUNCTION
 #define KOKKOS_LAMBDA [=]
+#define KOKKOS_CLASS_LAMBDA [=, *this]
 #define KOKKOS_ASSERT(x) ((void)0)
 #define YAKL_INLINE inline
 #define YAKL_LAMBDA [=]
@@ -143,6 +146,16 @@ void parallel_reduce(const RangePolicy<Space>& p, const F& f, const Reducer& r) 
     r.ref = result;
 }
 
+// Kokkos::abort stand-in: the oracle must not end the test process, so a
+// call is counted (moracle_abort_count) and the calling loop body goes on.
+inline std::atomic<long long>& abort_count() {
+    static std::atomic<long long> n{0};
+    return n;
+}
+inline void abort(const char*) {
+    abort_count().fetch_add(1);
+}
+
 } // namespace Kokkos
 
 namespace yakl {
@@ -157,7 +170,16 @@ struct DimsT {
     explicit DimsT(const X&) {}
 };
 
-struct SimpleNetCDF {};
+// NetCDF reader stand-in: the oracle never reads files (its EOS tables are
+// set in code), so every call is a no-op.
+constexpr int NETCDF_MODE_READ = 0;
+constexpr int NETCDF_MODE_WRITE = 1;
+struct SimpleNetCDF {
+    void open(const std::string&, int) {}
+    void close() {}
+    template <class T>
+    void read(T&, const std::string&) {}
+};
 
 inline void timer_start(const std::string&) {}
 inline void timer_stop(const std::string&) {}
