@@ -148,6 +148,19 @@ mc_status mc_destroy(mc_ctx* ctx);
  * when any active face is MC_BC_USERFN. fn = NULL removes the hook. */
 mc_status mc_set_user_bc(mc_ctx* ctx, void (*fn)(void* user, double* Q, void* stream), void* user);
 
+/* Domain-wide CFL minimum for a grid split over ranks. compute_dt reduces
+ * over the whole domain (source/Hydro.cpp:209-229); when each rank holds one
+ * part, the ranks' minima must be combined before dt is formed. fn is a host
+ * function that enqueues on `stream` that combination, in place, for the
+ * device word `cfl_min_bits`: the bit pattern of the non-negative CFL
+ * minimum, so a 64-bit integer MIN over the ranks is the minimum of the
+ * values. The library calls it wherever it forms a dt: in mc_compute_dt,
+ * and in mc_advance before every step's dt, so a device-driven loop needs no
+ * host round trip per step. fn = NULL removes it. No counterpart in the
+ * reference, which runs on one domain. */
+mc_status mc_set_cfl_reduce_hook(mc_ctx* ctx, void (*fn)(void* user, uint64_t* cfl_min_bits, void* stream),
+                                 void* user);
+
 /* ---- Non-ideal equations of state --------------------------------------------
  *
  * The EOS kinds of the reference (EosType ordinals, source/Eos.hpp:16-21);

@@ -75,6 +75,8 @@ class McBatchProblem(ctypes.Structure):
 
 
 USER_BC_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
+# void (*)(void* user, uint64_t* cfl_min_bits, void* stream)
+CFL_REDUCE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
 
 
 class McEosTable(ctypes.Structure):
@@ -147,6 +149,8 @@ def load() -> ctypes.CDLL:
     lib.mc_batch_schedule.restype = i32
     lib.mc_time_step_noalloc.argtypes = [P(McGrid), P(McScheme), vp, d, vp]
     lib.mc_time_step_noalloc.restype = i32
+    lib.mc_set_cfl_reduce_hook.argtypes = [vp, CFL_REDUCE_FN, vp]
+    lib.mc_set_cfl_reduce_hook.restype = i32
     lib.mc_set_gravity.argtypes = [vp, i32, d, d, d]
     lib.mc_set_gravity.restype = i32
     lib.mc_set_eos.argtypes = [vp, i32, d, i32, P(McEosTable)]

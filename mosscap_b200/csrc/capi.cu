@@ -35,6 +35,8 @@ struct mc_ctx {
     bool min_from_clock = false;  // last CFL minimum sits in blk->last_cfl_min
     void (*user_bc)(void*, double*, void*) = nullptr;
     void* user_bc_data = nullptr;
+    void (*cfl_hook)(void*, uint64_t*, void*) = nullptr;  // mc_set_cfl_reduce_hook
+    void* cfl_hook_data = nullptr;
     int gravity = 0;              // mc_set_gravity
     double grav[3] = {0.0, 0.0, 0.0};
     // non-ideal EOS (mc_set_eos)
@@ -250,6 +252,13 @@ mc_status enqueue_step(mc_ctx* c, double* Q, double dt, const double* dt_dev, bo
     return MC_OK;
 }
 
+// The caller's domain-wide reduction of the CFL minimum word, if any.
+void reduce_cfl(mc_ctx* c, cudaStream_t s) {
+    if (c->cfl_hook) {
+        c->cfl_hook(c->cfl_hook_data, reinterpret_cast<uint64_t*>(&c->blk->cfl_min_bits), (void*)s);
+    }
+}
+
 double clamp_to_output(double dt, const mc_clock* k) {
     // source/Hydro.cpp:231-241
     const double cand = k->prev_output_time + k->output_delta;
@@ -438,6 +447,15 @@ mc_status mc_set_gravity(mc_ctx* c, int32_t enabled, double gx, double gy, doubl
     return MC_OK;
 }
 
+mc_status mc_set_cfl_reduce_hook(mc_ctx* c, void (*fn)(void*, uint64_t*, void*), void* user) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    c->cfl_hook = fn;
+    c->cfl_hook_data = user;
+    return MC_OK;
+}
+
 mc_status mc_set_eos(mc_ctx* c, int32_t type, double avg_mass, int32_t include_ionisation_energy,
                      const mc_eos_table* t) {
     if (mc_status st = check_ctx(c)) {
@@ -552,6 +570,7 @@ mc_status mc_compute_dt(mc_ctx* c, const double* Q, const mc_clock* clock, doubl
     p.q_in = Q;
     c->launches += 2;
     MC_CUDA(mc::launch_cfl_min(p, c->grid.num_dim, s), "cfl_min");
+    reduce_cfl(c, s);
     MC_CUDA(cudaMemcpyAsync(c->blk_host, c->blk, sizeof(mc::DeviceBlock), cudaMemcpyDeviceToHost, s), "read-back");
     MC_CUDA(cudaStreamSynchronize(s), "sync");
     double m;
@@ -608,6 +627,7 @@ mc_status mc_advance(mc_ctx* c, double* Q, mc_clock* clock, int64_t max_steps, i
     StageParams p = base_params(c);
     p.q_in = Q;
     MC_CUDA(mc::launch_cfl_min(p, c->grid.num_dim, s), "cfl_min");
+    reduce_cfl(c, s);
     MC_CUDA(mc::launch_clock_advance(c->blk, dlog, 1, s), "clock");
     c->launches += 4;
     const double* dt_dev = &c->blk->dt;
@@ -619,6 +639,7 @@ mc_status mc_advance(mc_ctx* c, double* Q, mc_clock* clock, int64_t max_steps, i
             if (mc_status st = enqueue_step(c, Q, 0.0, dt_dev, false, s)) {
                 return st;
             }
+            reduce_cfl(c, s);
             MC_CUDA(mc::launch_clock_advance(c->blk, dlog, 0, s), "clock");
             c->launches += 1;
         }

@@ -14,7 +14,10 @@ output times as ``compute_dt`` does (source/Hydro.cpp:231-241). A slab run
 is therefore bit-identical to the single-domain run.
 
 The outer y faces keep the global problem's kinds; periodic outer faces are
-exchanged between the last and the first rank.
+exchanged between the last and the first rank. ``SlabSim.advance`` runs the
+device-driven loop instead: the global CFL minimum is then an in-stream
+all-reduce through the library's CFL reduce hook (``mc_set_cfl_reduce_hook``)
+and no step waits for the host.
 """
 from __future__ import annotations
 
@@ -35,8 +38,8 @@ from .problems import Problem
 class _CudaArray:
     """A raw device pointer exposed through __cuda_array_interface__."""
 
-    def __init__(self, ptr: int, shape):
-        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8", "data": (int(ptr), False),
+    def __init__(self, ptr: int, shape, typestr: str = "<f8"):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
                                          "version": 3, "strides": None}
 
 
@@ -129,6 +132,17 @@ class SlabSim:
         self._hook = capi.USER_BC_FN(self._fill_rows)
         capi.check(self.sim.lib.mc_set_user_bc(self.sim.ctx, self._hook, None), "mc_set_user_bc")
         self._fused_min_valid = False
+        # the domain-wide CFL minimum of the device-driven loop: an in-stream
+        # all-reduce MIN of the 64-bit word holding the bits of the
+        # non-negative minimum (integer order = value order)
+        self._reduce = capi.CFL_REDUCE_FN(self._reduce_min)
+        if world > 1:
+            capi.check(self.sim.lib.mc_set_cfl_reduce_hook(self.sim.ctx, self._reduce, None),
+                       "mc_set_cfl_reduce_hook")
+
+    def _reduce_min(self, user, ptr, stream):
+        word = torch.as_tensor(_CudaArray(ptr, (1,), "<i8"), device=self.sim.device)
+        dist.all_reduce(word, op=dist.ReduceOp.MIN, group=self.group)
 
     def _fill_rows(self, user, qptr, stream):
         shape = tuple(self.sim.Q.shape)
@@ -157,6 +171,14 @@ class SlabSim:
             local = float(t.item())
         s = self.sim
         return clamp_to_output(local, s.time, s.max_time, s.prev_output_time, s.output_delta)
+
+    def advance(self, max_steps: int):
+        """Up to max_steps steps in the device-driven loop (mc_advance): ghost
+        rows through the boundary hook after every stage, the global CFL
+        minimum through the reduce hook before every dt; no host round trip
+        per step. Returns the dt of each step."""
+        self._fused_min_valid = False
+        return self.sim.advance(max_steps)
 
     def step(self) -> float:
         dt = self.compute_dt()

@@ -74,3 +74,39 @@ def test_clamp_to_output_matches_reference_rule():
     # clamped to max_time
     dt = clamp_to_output(0.5, 0.9, 1.0, 0.0, 5.0)
     assert 0.9 + dt >= 1.0
+
+
+def _min_worker(rank, world, port, errors):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rng = np.random.default_rng(7)
+        vals = np.concatenate([rng.uniform(0.0, 1e-3, size=(world, 64)), np.zeros((world, 1)),
+                               np.full((world, 1), np.inf), 10.0 ** rng.uniform(-300, 300, size=(world, 64))], axis=1)
+        mine = vals[rank]
+        # what the CFL reduce hook of SlabSim does to the library's word: an
+        # integer MIN over the bit patterns of the non-negative minima
+        word = torch.from_numpy(mine.view(np.int64).copy())
+        dist.all_reduce(word, op=dist.ReduceOp.MIN)
+        got = word.numpy().view(np.float64)
+        if not np.array_equal(got, vals.min(axis=0)):
+            errors.put(f"rank {rank}: integer MIN of the bits is not the minimum")
+    finally:
+        dist.destroy_process_group()
+
+
+def test_cfl_minimum_by_integer_min_of_bits():
+    """The slab decomposition's global CFL minimum is an all-reduce MIN of
+    the 64-bit words holding the bits of each rank's non-negative minimum
+    (zero and +inf included): integer order equals value order."""
+    ctx = mp.get_context("spawn")
+    errors = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_min_worker, args=(r, 3, port, errors)) for r in range(3)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert errors.empty(), errors.get()

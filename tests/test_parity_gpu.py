@@ -186,6 +186,62 @@ def test_fp32_form_error_bounds(gpu_lib, oracle_port):
     assert sim.status() == 0
 
 
+def test_slab_decomposition_device_loop_single_rank(gpu_lib, oracle_port):
+    """The slab path in the device-driven loop (SlabSim.advance) on one rank
+    is bit-identical to the reference run of the same periodic problem."""
+    from mosscap_b200.distributed import SlabSim
+    p = P.kelvin_helmholtz_2d(96, seed=6)
+    o = _oracle(oracle_port, p)
+    ref_dts = o.run(8)
+    s = SlabSim(p, rank=0, world=1)
+    s.fill_bcs()
+    dts = s.advance(8)
+    _assert_same(np.array(dts), ref_dts, "dt")
+    _assert_same(s.sim.get_Q(), o.get_Q(), "state")
+
+
+def test_cfl_reduce_hook(gpu_lib):
+    """mc_set_cfl_reduce_hook: called once before every dt of the device loop
+    (and by mc_compute_dt), in-stream, on the word the dt is formed from."""
+    import ctypes
+    import torch
+    from mosscap_b200 import capi
+    from mosscap_b200.distributed import _CudaArray
+    from mosscap_b200.hydro import HydroSim
+    p = P.kelvin_helmholtz_2d(64, seed=2)
+    base = HydroSim(p)
+    base.fill_bcs()
+    ref = base.advance(6)
+    calls = []
+
+    def count(user, ptr, stream):
+        calls.append(ptr)
+
+    sim = HydroSim(p)
+    sim.fill_bcs()
+    hook = capi.CFL_REDUCE_FN(count)
+    capi.check(sim.lib.mc_set_cfl_reduce_hook(sim.ctx, hook, None), "hook")
+    dts = sim.advance(6)
+    assert len(calls) == 7
+    _assert_same(dts, ref, "dt with an identity hook")
+    # a hook that caps the minimum: every dt follows the capped value
+    cap = 0.5 * ref[0] / p.max_cfl
+    cap_bits = int(np.array([cap]).view(np.int64)[0])
+
+    def capper(user, ptr, stream):
+        w = torch.as_tensor(_CudaArray(ptr, (1,), "<i8"), device="cuda")
+        torch.clamp_(w, max=cap_bits)
+
+    sim2 = HydroSim(p)
+    sim2.fill_bcs()
+    hook2 = capi.CFL_REDUCE_FN(capper)
+    capi.check(sim2.lib.mc_set_cfl_reduce_hook(sim2.ctx, hook2, None), "hook")
+    dts2 = sim2.advance(4)
+    assert dts2[0] == cap * p.max_cfl and (dts2 <= cap * p.max_cfl).all()
+    assert sim2.compute_dt() <= cap * p.max_cfl
+    capi.check(sim2.lib.mc_set_cfl_reduce_hook(sim2.ctx, capi.CFL_REDUCE_FN(0), None), "unhook")
+
+
 def test_slab_decomposition_single_rank(gpu_lib, oracle_port):
     """The slab path (y faces filled by the boundary hook, dt from the
     step's fused CFL minimum) on one rank with a self-periodic exchange is
