@@ -338,9 +338,6 @@ mc_status mc_create(const mc_grid* grid, const mc_scheme* scheme, mc_ctx** out) 
     if (g.num_tracers < 0 || 2 + g.num_dim + g.num_tracers > mc::kMaxVars) {
         return fail(MC_ERR_INVALID_ARGUMENT, "too many variables (at most 8)");
     }
-    if (g.num_dim == 3 && g.num_tracers > 0) {
-        return fail(MC_ERR_UNSUPPORTED, "passive tracers are not implemented in 3D");
-    }
     if (!(g.dx > 0.0) || !std::isfinite(g.dx) || !std::isfinite(s.gamma) || !std::isfinite(s.max_cfl)) {
         return fail(MC_ERR_INVALID_ARGUMENT, "dx, gamma and max_cfl must be finite (dx > 0)");
     }

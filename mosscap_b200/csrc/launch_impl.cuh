@@ -72,9 +72,12 @@ cudaError_t launch_one(const StageParams& p, int pass, cudaStream_t s) {
         }
         k<<<dim3(cdiv(p.nx, kTile), cdiv(p.ny, kTile), p.nz), dim3(kThreads), sm, s>>>(p);
     } else {
-        zsweep3d_kernel<REC, LIM, RS, Real, MC_SRC>
-            <<<dim3(cdiv(p.nx, kZBlockX), cdiv(p.ny, kZBlockY), cdiv(p.nz, kZChunk)), dim3(kZBlockX, kZBlockY), 0,
-               s>>>(p);
+        const dim3 g(cdiv(p.nx, kZBlockX), cdiv(p.ny, kZBlockY), cdiv(p.nz, kZChunk)), b(kZBlockX, kZBlockY);
+        if (p.ntracer > 0) {
+            zsweep3d_kernel<REC, LIM, RS, Real, MC_SRC, kMaxVars - 5><<<g, b, 0, s>>>(p);
+        } else {
+            zsweep3d_kernel<REC, LIM, RS, Real, MC_SRC, 0><<<g, b, 0, s>>>(p);
+        }
     }
 #endif
     return cudaGetLastError();

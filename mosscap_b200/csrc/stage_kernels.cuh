@@ -444,6 +444,12 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
                     qu += double(dfy[v * YV]);
                     p.dqxy[v * cells + o] = qu;
                 }
+                for (int t = 0; t < ntr; ++t) {
+                    double qu = 0.0;
+                    qu += double(d_tr[t]);
+                    qu += double(dfy[(nh + t) * YV]);
+                    p.dqxy[(nh + t) * cells + o] = qu;
+                }
             } else {
                 double qn[kMaxVars];
 #pragma unroll
@@ -497,7 +503,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : k
 // 3D z pass: one thread per interior (x, y) column, marching along z over a
 // chunk of kZChunk cells with a register window of primitives. Adds the z
 // divergence to the x+y divergence from the plane pass and finishes the
-// stage. No passive tracers.
+// stage. Passive tracers (up to kMaxVars - 5) in the NTR instantiation.
 // ---------------------------------------------------------------------------
 constexpr int kZChunk = 32;
 constexpr int kZBlockX = 32, kZBlockY = 4;
@@ -506,8 +512,8 @@ constexpr int kZBlockX = 32, kZBlockY = 4;
 // latency-bound, and 16 resident warps with a few spilled registers measured
 // 7 % faster on Sedov 512^3 than 12 warps without spills (168 registers);
 // loading the next window cell one step ahead gained nothing.
-template <int REC, int LIM, int RS, class T, bool SRC = false>
-__global__ void __launch_bounds__(kZBlockX* kZBlockY, 4) zsweep3d_kernel(StageParams p) {
+template <int REC, int LIM, int RS, class T, bool SRC = false, int NTR = 0>
+__global__ void __launch_bounds__(kZBlockX* kZBlockY, NTR > 0 ? 2 : 4) zsweep3d_kernel(StageParams p) {
     if (p.dt_dev && p.blk->done) {
         return;
     }
@@ -516,6 +522,7 @@ __global__ void __launch_bounds__(kZBlockX* kZBlockY, 4) zsweep3d_kernel(StagePa
     constexpr int nh = 5;
     constexpr int S = stencil_half<REC>();
     constexpr int WN = 2 * S + 1;  // window length
+    constexpr int TS = NTR > 0 ? NTR : 1;  // tracer slots compiled in (p.ntracer <= NTR used)
     __shared__ double red_d[kWarps];
     __shared__ unsigned red_u[kWarps];
     const int xi = blockIdx.x * kZBlockX + threadIdx.x;
@@ -529,11 +536,17 @@ __global__ void __launch_bounds__(kZBlockX* kZBlockY, 4) zsweep3d_kernel(StagePa
     const double dt = stage_dt(p);
     const double dtdx = dt / p.dx;
     const long long cells = (long long)p.nx * p.ny * p.nz;
+    const int ntr = NTR > 0 ? p.ntracer : 0;
     unsigned flags = 0;
     double dtmin = __longlong_as_double(0x7ff0000000000000ll);
 
     if (active) {
-        auto load_w = [&](int zc_interior, T* w) {
+        // window[o][v] holds the primitives of cell (zc - S + o) where zc is
+        // the cell being reconstructed; wt[o][t] its tracers scaled to mass
+        // fractions (source/Hydro.cpp:27-33)
+        T win[WN][nh];
+        T wt[WN][TS];
+        auto load_w = [&](int zc_interior, int slot) {
             double q[nh], wd[nh];
             const int kk = zc_interior + p.ng;
 #pragma unroll
@@ -545,19 +558,23 @@ __global__ void __launch_bounds__(kZBlockX* kZBlockY, 4) zsweep3d_kernel(StagePa
 #pragma unroll
             for (int v = 0; v < nh; ++v) {
                 fin = fin && isfinite(q[v]);
-                w[v] = T(wd[v]);
+                win[slot][v] = T(wd[v]);
+            }
+            if constexpr (NTR > 0) {
+                const double inv_rho = 1.0 / q[0];
+#pragma unroll
+                for (int t = 0; t < NTR; ++t) {
+                    wt[slot][t] = t < ntr ? T(p.q_in[qidx(p, nh + t, kk, j, i)] * inv_rho) : T(0);
+                }
             }
             return state_flags(wd[0], wd[nh - 1], fin);
         };
-        // window[o][v] holds the primitives of cell (zc - S + o) where zc is
-        // the cell being reconstructed
-        T win[WN][nh];
         // cells z0-1-S .. z0-1+S for the reconstruction of cell z0-1
 #pragma unroll
         for (int o = 0; o < WN; ++o) {
-            flags |= load_w(z0 - 1 - S + o, win[o]);
+            flags |= load_w(z0 - 1 - S + o, o);
         }
-        auto recon_window = [&](T* rl, T* rr) {
+        auto recon_window = [&](T* rl, T* rr, T* tl, T* tr) {
 #pragma unroll
             for (int v = 0; v < nh; ++v) {
                 T s[5];
@@ -567,6 +584,17 @@ __global__ void __launch_bounds__(kZBlockX* kZBlockY, 4) zsweep3d_kernel(StagePa
                 }
                 reconstruct<REC, LIM>(s, rl[v], rr[v]);
             }
+            if constexpr (NTR > 0) {
+#pragma unroll
+                for (int t = 0; t < NTR; ++t) {
+                    T s[5];
+#pragma unroll
+                    for (int o = 0; o < WN; ++o) {
+                        s[2 - S + o] = wt[o][t];
+                    }
+                    reconstruct<REC, LIM>(s, tl[t], tr[t]);
+                }
+            }
         };
         auto shift_in = [&](int zc_interior) {
 #pragma unroll
@@ -575,25 +603,48 @@ __global__ void __launch_bounds__(kZBlockX* kZBlockY, 4) zsweep3d_kernel(StagePa
                 for (int v = 0; v < nh; ++v) {
                     win[o][v] = win[o + 1][v];
                 }
+                if constexpr (NTR > 0) {
+#pragma unroll
+                    for (int t = 0; t < NTR; ++t) {
+                        wt[o][t] = wt[o + 1][t];
+                    }
+                }
             }
-            flags |= load_w(zc_interior, win[WN - 1]);
+            flags |= load_w(zc_interior, WN - 1);
+        };
+        // tracer flux of a face: upwinded by the sign of the mass flux
+        // (source/Hydro.cpp:155-162)
+        auto tracer_flux = [&](const T* f, const T* tleft, const T* tright, T* ft) {
+            if constexpr (NTR > 0) {
+#pragma unroll
+                for (int t = 0; t < NTR; ++t) {
+                    ft[t] = (f[0] >= T(0)) ? f[0] * tleft[t] : f[0] * tright[t];
+                }
+            }
         };
         T rr_prev[nh], rl_cur[nh], rr_cur[nh], f_prev[nh], f_cur[nh];
+        T tr_prev[TS], tl_cur[TS], tr_cur[TS], ft_prev[TS], ft_cur[TS];
         {
-            T rl_tmp[nh];
-            recon_window(rl_tmp, rr_prev);  // cell z0-1
+            T rl_tmp[nh], tl_tmp[TS];
+            recon_window(rl_tmp, rr_prev, tl_tmp, tr_prev);  // cell z0-1
         }
         shift_in(z0 + S);
-        recon_window(rl_cur, rr_cur);  // cell z0
+        recon_window(rl_cur, rr_cur, tl_cur, tr_cur);  // cell z0
         riemann<RS, NDIM>(gamma, gfac, 2, rr_prev, rl_cur, f_prev);  // face z0 - 1/2
+        tracer_flux(f_prev, tr_prev, tl_cur, ft_prev);
 #pragma unroll
         for (int v = 0; v < nh; ++v) {
             rr_prev[v] = rr_cur[v];
         }
+#pragma unroll
+        for (int t = 0; t < TS; ++t) {
+            tr_prev[t] = tr_cur[t];
+        }
         for (int z = z0; z < z1; ++z) {
             shift_in(z + 1 + S);
-            recon_window(rl_cur, rr_cur);  // cell z+1
+            recon_window(rl_cur, rr_cur, tl_cur, tr_cur);  // cell z+1
             riemann<RS, NDIM>(gamma, gfac, 2, rr_prev, rl_cur, f_cur);  // face z + 1/2
+            tracer_flux(f_cur, tr_prev, tl_cur, ft_cur);
             const int kk = z + p.ng;
             const long long o = ((long long)z * p.ny + yi) * p.nx + xi;
             double qn[kMaxVars];
@@ -603,20 +654,38 @@ __global__ void __launch_bounds__(kZBlockX* kZBlockY, 4) zsweep3d_kernel(StagePa
             }
             double sdt[nh];
             source_dt<NDIM, SRC>(p, kk, j, i, dt, sdt);
+            const bool old = combo_reads_old(p.combo);
 #pragma unroll
             for (int v = 0; v < nh; ++v) {
                 double qu = p.dqxy[v * cells + o];
                 qu += double(f_prev[v] - f_cur[v]);
                 qu *= dtdx;
                 const long long id = qidx(p, v, kk, j, i);
-                const double qo = combo_reads_old(p.combo) ? p.q_old[id] : 0.0;
+                const double qo = old ? p.q_old[id] : 0.0;
                 qn[v] = combine(p.combo, qo, p.q_in[id], qu, sdt[v]);
+            }
+            if constexpr (NTR > 0) {
+#pragma unroll
+                for (int t = 0; t < NTR; ++t) {
+                    if (t < ntr) {
+                        double qu = p.dqxy[(nh + t) * cells + o];
+                        qu += double(ft_prev[t] - ft_cur[t]);
+                        qu *= dtdx;
+                        const long long id = qidx(p, nh + t, kk, j, i);
+                        qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0);
+                    }
+                }
             }
             dtmin = smin(write_cell<NDIM>(p, i, j, kk, qn, p.last != 0, &flags), dtmin);
 #pragma unroll
             for (int v = 0; v < nh; ++v) {
                 f_prev[v] = f_cur[v];
                 rr_prev[v] = rr_cur[v];
+            }
+#pragma unroll
+            for (int t = 0; t < TS; ++t) {
+                ft_prev[t] = ft_cur[t];
+                tr_prev[t] = tr_cur[t];
             }
         }
     }

@@ -10,9 +10,10 @@ synthetic inputs and records:
   for the three headline workloads at fixture size (Sod 1D at full size, KH 2D
   at 64^2, Sedov 3D at 12^3);
 * ``sweep.json`` -- for every reconstruction x limiter x Riemann solver x
-  stepper on small 1D / 2D / 3D grids with mixed boundary kinds, and for the
-  gravity source term with every stepper, the SHA-256 of the input and of the
-  final state and the dt sequence (bit patterns).
+  stepper on small 1D / 2D / 3D grids with mixed boundary kinds, for the
+  gravity source term with every stepper, and for two passive tracers in 3D,
+  the SHA-256 of the input and of the final state and the dt sequence (bit
+  patterns).
 
 Run from the repository root:  python tests/golden/make_golden.py
 """
@@ -101,6 +102,17 @@ def sweep_cases():
                       dx=1.0 / n, bc=SWEEP_BCS[ndim], reconstruction=rec, slope_limiter=lim, riemann_solver="hllc",
                       time_stepper=st, gamma=1.4, max_cfl=0.6, max_time=0.04, output_delta=0.015,
                       gravity=(-1.5, 0.75, -0.5), Q=q)
+        out.append((p.name, p, 6, seed))
+    # passive tracers in 3D (two fields) with each reconstruction, HLL / HLLC
+    # and rk2 / ssprk3
+    for (rec, lim), rs, st in itertools.product([SWEEP_RECON[0], SWEEP_RECON[2], SWEEP_RECON[5], SWEEP_RECON[7]],
+                                                 ("hll", "hllc"), ("rk2", "ssprk3")):
+        n = SWEEP_N[3]
+        seed = 7000 + 17 * SWEEP_RECON.index((rec, lim)) + 5 * ("hll", "hllc").index(rs) + ("rk2", "ssprk3").index(st)
+        q = P.random_state(3, n, n, n, ng=3, num_tracers=2, seed=seed)
+        p = P.Problem(f"tracer3d_{rec}_{lim}_{rs}_{st}", 3, n, n, n, ng=3, num_tracers=2, dx=1.0 / n,
+                      bc=SWEEP_BCS[3], reconstruction=rec, slope_limiter=lim, riemann_solver=rs, time_stepper=st,
+                      gamma=1.4, max_cfl=0.6, max_time=0.04, output_delta=0.015, Q=q)
         out.append((p.name, p, 6, seed))
     return out
 

@@ -60,7 +60,7 @@ def test_sweep_fixture(kind, request):
         assert [int(x) for x in _bits(dts)] == g["dt_bits"], name
         assert _sha(q1) == g["q1_sha256"], name
         n += 1
-    assert n == len(gold) == 225
+    assert n == len(gold) == 241
 
 
 def test_constant_boundaries_port_vs_reference(oracle_port, oracle_ref):
