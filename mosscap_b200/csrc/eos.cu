@@ -106,7 +106,8 @@ struct Sample {
     double y, log_T;
 };
 
-__device__ __forceinline__ Sample table_sample(const EosLaunch& L, double log_eint_rho, double log_rho) {
+__device__ __forceinline__ Sample table_sample(const EosLaunch& L, const double* Y, const double* LT,
+                                              double log_eint_rho, double log_rho) {
     const double frac_eint_rho = (log_eint_rho - L.x_start) / L.x_step;
     int ix = int(floor(frac_eint_rho));
     int ixp;
@@ -140,8 +141,6 @@ __device__ __forceinline__ Sample table_sample(const EosLaunch& L, double log_ei
         ty = 1.0 - typ;
     }
     const int n = L.nx_tab;
-    const double* Y = L.y_table;
-    const double* LT = L.log_T_table;
     Sample s;
     s.y = (ty * (tx * Y[iy * n + ix] + txp * Y[iy * n + ixp]) + typ * (tx * Y[iyp * n + ix] + txp * Y[iyp * n + ixp]));
     s.log_T = (ty * (tx * LT[iy * n + ix] + txp * LT[iy * n + ixp]) +
@@ -149,47 +148,103 @@ __device__ __forceinline__ Sample table_sample(const EosLaunch& L, double log_ei
     return s;
 }
 
+// With tables_in_smem, a persistent grid whose CTAs first copy both tables
+// into shared memory: each cell then gathers its eight table values from
+// shared memory instead of waiting on global loads after its state loads.
 template <int NDIM>
-__global__ void __launch_bounds__(256) eos_tabulated_kernel(EosLaunch L) {
+__global__ void __launch_bounds__(256) eos_tabulated_kernel(EosLaunch L, int tables_in_smem) {
     if (L.blk && L.skip_when_done && L.blk->done) {
         return;
     }
-    constexpr int ie = 1 + NDIM;
-    unsigned flags = 0;
-    for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < L.plane;
-         id += (long long)gridDim.x * blockDim.x) {
-        double rho, e_kin, eint;
-        energies<NDIM>(L.q_in, id, L.plane, rho, e_kin, eint);
-        const double log_rho = log10(rho);
-        const double log_eint_rho = log10(eint) - log_rho;
-        // The reference aborts on eint < 0 (TabulatedLteH.hpp:142-144); a
-        // NaN coordinate (eint < 0, rho <= 0 or a non-finite state) would
-        // also index the table out of range. Flag the cell and leave it.
-        const double fx = (log_eint_rho - L.x_start) / L.x_step;
-        const double fy = (log_rho - L.y_start) / L.y_step;
-        if (eint < 0.0 || fx != fx || fy != fy) {
-            flags |= kFlagEos;
-            continue;
+    extern __shared__ __align__(16) double tab_smem[];
+    const double* Y = L.y_table;
+    const double* LT = L.log_T_table;
+    if (tables_in_smem) {
+        const int n = L.nx_tab * L.ny_tab;
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            tab_smem[k] = L.y_table[k];
+            tab_smem[n + k] = L.log_T_table[k];
         }
-        const Sample s = table_sample(L, log_eint_rho, log_rho);
-        const double prev_y = L.y[id];
-        L.y[id] = s.y;
-        const double delta_eint = (prev_y < 0.0) ? 0.0 : rho * (kChiH / kHMass) * (s.y - prev_y);
-        L.T[id] = pow(10.0, s.log_T);
-        // the state with the energy shifted: in place, or into a copy when
-        // the input must stay as it is (the step-start state)
-        if (L.q_out != L.q_in) {
-            for (int v = 0; v < L.nvar; ++v) {
-                if (v != ie) {
-                    L.q_out[id + v * L.plane] = L.q_in[id + v * L.plane];
+        __syncthreads();
+        Y = tab_smem;
+        LT = tab_smem + n;
+    }
+    constexpr int ie = 1 + NDIM;
+    constexpr int nh = 2 + NDIM;
+    constexpr int U = 4;  // cells per thread whose loads are issued together
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    unsigned flags = 0;
+    for (long long base = blockIdx.x * (long long)blockDim.x + threadIdx.x; base < L.plane; base += U * stride) {
+        double qv[U][nh], yp[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long id = base + u * stride;
+            if (id < L.plane) {
+#pragma unroll
+                for (int v = 0; v < nh; ++v) {
+                    qv[u][v] = L.q_in[id + v * L.plane];
                 }
+                yp[u] = L.y[id];
             }
         }
-        L.q_out[id + ie * L.plane] = L.q_in[id + ie * L.plane] + delta_eint;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long id = base + u * stride;
+            if (id >= L.plane) {
+                continue;
+            }
+            const double* q = qv[u];
+            double mom2_sum = q[1] * q[1];
+            if constexpr (NDIM > 1) {
+                mom2_sum += q[2] * q[2];
+            }
+            if constexpr (NDIM > 2) {
+                mom2_sum += q[3] * q[3];
+            }
+            const double rho = q[0];
+            const double e_kin = 0.5 * mom2_sum / rho;
+            const double eint = q[ie] - e_kin;
+            const double log_rho = log10(rho);
+            const double log_eint_rho = log10(eint) - log_rho;
+            // The reference aborts on eint < 0 (TabulatedLteH.hpp:142-144); a
+            // NaN coordinate (eint < 0, rho <= 0 or a non-finite state) would
+            // also index the table out of range. Flag the cell and leave it.
+            const double fx = (log_eint_rho - L.x_start) / L.x_step;
+            const double fy = (log_rho - L.y_start) / L.y_step;
+            if (eint < 0.0 || fx != fx || fy != fy) {
+                flags |= kFlagEos;
+                continue;
+            }
+            const Sample s = table_sample(L, Y, LT, log_eint_rho, log_rho);
+            const double prev_y = yp[u];
+            L.y[id] = s.y;
+            const double delta_eint = (prev_y < 0.0) ? 0.0 : rho * (kChiH / kHMass) * (s.y - prev_y);
+            L.T[id] = pow(10.0, s.log_T);
+            // the state with the energy shifted: in place, or into a copy when
+            // the input must stay as it is (the step-start state)
+            if (L.q_out != L.q_in) {
+                for (int v = 0; v < L.nvar; ++v) {
+                    if (v != ie) {
+                        L.q_out[id + v * L.plane] = L.q_in[id + v * L.plane];
+                    }
+                }
+            }
+            L.q_out[id + ie * L.plane] = q[ie] + delta_eint;
+        }
     }
     if (flags && L.blk) {
         atomicOr(&L.blk->status, flags);
     }
+}
+
+constexpr size_t kTableSmemMax = 74 * 1024;  // three CTAs per SM (228 KB)
+
+template <class K>
+cudaError_t allow_table_smem(K kernel, size_t bytes) {
+    if (bytes <= 48 * 1024) {
+        return cudaSuccess;
+    }
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 } // namespace
@@ -206,12 +261,24 @@ cudaError_t launch_eos_update(const EosLaunch& L, int ndim, cudaStream_t s) {
             eos_analytic_kernel<3><<<blocks, 256, 0, s>>>(L);
         }
     } else if (L.type == kEosTabulated) {
+        // both tables in shared memory when they fit three CTAs per SM
+        const size_t tab_bytes = 2 * sizeof(double) * (size_t)L.nx_tab * (size_t)L.ny_tab;
+        const bool smem = tab_bytes <= kTableSmemMax;
+        const size_t sm = smem ? tab_bytes : 0;
+        const int grid = smem ? (int)(want < 148 * 3 ? want : 148 * 3) : blocks;
+        cudaError_t e = cudaSuccess;
         if (ndim == 1) {
-            eos_tabulated_kernel<1><<<blocks, 256, 0, s>>>(L);
+            e = allow_table_smem(eos_tabulated_kernel<1>, sm);
+            eos_tabulated_kernel<1><<<grid, 256, sm, s>>>(L, smem ? 1 : 0);
         } else if (ndim == 2) {
-            eos_tabulated_kernel<2><<<blocks, 256, 0, s>>>(L);
+            e = allow_table_smem(eos_tabulated_kernel<2>, sm);
+            eos_tabulated_kernel<2><<<grid, 256, sm, s>>>(L, smem ? 1 : 0);
         } else {
-            eos_tabulated_kernel<3><<<blocks, 256, 0, s>>>(L);
+            e = allow_table_smem(eos_tabulated_kernel<3>, sm);
+            eos_tabulated_kernel<3><<<grid, 256, sm, s>>>(L, smem ? 1 : 0);
+        }
+        if (e != cudaSuccess) {
+            return e;
         }
     }
     return cudaGetLastError();
