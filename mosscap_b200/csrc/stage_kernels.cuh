@@ -508,12 +508,15 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : k
 constexpr int kZChunk = 32;
 constexpr int kZBlockX = 32, kZBlockY = 4;
 
-// Four CTAs of 128 threads per SM (up to 128 registers): the march is
-// latency-bound, and 16 resident warps with a few spilled registers measured
-// 7 % faster on Sedov 512^3 than 12 warps without spills (168 registers);
-// loading the next window cell one step ahead gained nothing.
+// The march is latency-bound. Each step loads the cell's own inputs of the
+// stage combination (x+y divergence, stage input, step-start state) before
+// the reconstruction and Riemann solve that precede their use, so those
+// loads overlap that arithmetic; with them, three CTAs of 128 threads per
+// SM (168 registers) measured 11 % faster on Sedov 512^3 than four CTAs
+// with the loads after the solve (128 registers, spilling). Loading the
+// next window cell one step ahead gained nothing.
 template <int REC, int LIM, int RS, class T, bool SRC = false, int NTR = 0>
-__global__ void __launch_bounds__(kZBlockX* kZBlockY, NTR > 0 ? 2 : 4) zsweep3d_kernel(StageParams p) {
+__global__ void __launch_bounds__(kZBlockX* kZBlockY, NTR > 0 ? 2 : 3) zsweep3d_kernel(StageParams p) {
     if (p.dt_dev && p.blk->done) {
         return;
     }
@@ -640,13 +643,25 @@ __global__ void __launch_bounds__(kZBlockX* kZBlockY, NTR > 0 ? 2 : 4) zsweep3d_
         for (int t = 0; t < TS; ++t) {
             tr_prev[t] = tr_cur[t];
         }
+        const bool old = combo_reads_old(p.combo);
         for (int z = z0; z < z1; ++z) {
+            const int kk = z + p.ng;
+            const long long o = ((long long)z * p.ny + yi) * p.nx + xi;
+            // the cell's own inputs of the stage combination are loaded
+            // before its reconstruction and Riemann solve, so their memory
+            // latency overlaps that arithmetic
+            double dq[nh], qi[nh], qo[nh];
+#pragma unroll
+            for (int v = 0; v < nh; ++v) {
+                const long long id = qidx(p, v, kk, j, i);
+                dq[v] = p.dqxy[v * cells + o];
+                qi[v] = p.q_in[id];
+                qo[v] = old ? p.q_old[id] : 0.0;
+            }
             shift_in(z + 1 + S);
             recon_window(rl_cur, rr_cur, tl_cur, tr_cur);  // cell z+1
             riemann<RS, NDIM>(gamma, gfac, 2, rr_prev, rl_cur, f_cur);  // face z + 1/2
             tracer_flux(f_cur, tr_prev, tl_cur, ft_cur);
-            const int kk = z + p.ng;
-            const long long o = ((long long)z * p.ny + yi) * p.nx + xi;
             double qn[kMaxVars];
 #pragma unroll
             for (int v = 0; v < kMaxVars; ++v) {
@@ -654,15 +669,12 @@ __global__ void __launch_bounds__(kZBlockX* kZBlockY, NTR > 0 ? 2 : 4) zsweep3d_
             }
             double sdt[nh];
             source_dt<NDIM, SRC>(p, kk, j, i, dt, sdt);
-            const bool old = combo_reads_old(p.combo);
 #pragma unroll
             for (int v = 0; v < nh; ++v) {
-                double qu = p.dqxy[v * cells + o];
+                double qu = dq[v];
                 qu += double(f_prev[v] - f_cur[v]);
                 qu *= dtdx;
-                const long long id = qidx(p, v, kk, j, i);
-                const double qo = old ? p.q_old[id] : 0.0;
-                qn[v] = combine(p.combo, qo, p.q_in[id], qu, sdt[v]);
+                qn[v] = combine(p.combo, qo[v], qi[v], qu, sdt[v]);
             }
             if constexpr (NTR > 0) {
 #pragma unroll
