@@ -90,18 +90,20 @@ __device__ __forceinline__ double stage_dt(const StageParams& p) {
 // the stage update adds S dt (source/TimeStepping.cpp:60-66). SRC is false
 // in the kernels launched without a source term: S stays 0 and the result is
 // 0 * dt.
+// This form takes the cell's stage-input state q[0..1+NDIM] from the caller.
 template <int NDIM, bool SRC>
-__device__ __forceinline__ void source_dt(const StageParams& p, int k, int j, int i, double dt, double* sdt) {
+__device__ __forceinline__ void source_dt_of(const StageParams& p, const double* qc, double dt, double* sdt) {
     constexpr int nh = 2 + NDIM;
     if constexpr (!SRC) {
+        (void)p;
+        (void)qc;
 #pragma unroll
         for (int v = 0; v < nh; ++v) {
             sdt[v] = 0.0 * dt;
         }
         return;
     }
-    (void)p.gravity;
-    auto q = [&](int v) { return p.q_in[(((long long)v * p.zc + k) * p.yc + j) * (long long)p.xc + i]; };
+    auto q = [&](int v) { return qc[v]; };
     const double rho = q(0);
     double S[nh];
     S[0] = 0.0;
@@ -122,6 +124,21 @@ __device__ __forceinline__ void source_dt(const StageParams& p, int k, int j, in
     }
 }
 
+template <int NDIM, bool SRC>
+__device__ __forceinline__ void source_dt(const StageParams& p, int k, int j, int i, double dt, double* sdt) {
+    constexpr int nh = 2 + NDIM;
+    double q[nh];
+#pragma unroll
+    for (int v = 0; v < nh; ++v) {
+        if constexpr (SRC) {
+            q[v] = p.q_in[(((long long)v * p.zc + k) * p.yc + j) * (long long)p.xc + i];
+        } else {
+            q[v] = 0.0;
+        }
+    }
+    source_dt_of<NDIM, SRC>(p, q, dt, sdt);
+}
+
 // One SSPRK stage update of one variable; qu is the flux divergence already
 // multiplied by dt/dx and src the source term times dt.
 __device__ __forceinline__ double combine(int combo, double q_old, double q_in, double qu, double src) {
@@ -138,6 +155,51 @@ __device__ __forceinline__ double combine(int combo, double q_old, double q_in, 
             return q_in + 0.5 * (qu + src);
         default:
             return (2.0 / 3.0) * q_old + (1.0 / 3.0) * q_in + (1.0 / 6.0) * (qu + src);
+    }
+}
+
+// combine() over the first N variables with one dispatch on the combination
+// (the same expression per variable).
+template <int N>
+__device__ __forceinline__ void combine_all(int combo, const double* q_old, const double* q_in, const double* qu,
+                                            const double* src, double* out) {
+    switch (combo) {
+        case kAdd:
+#pragma unroll
+            for (int v = 0; v < N; ++v) {
+                out[v] = combine(kAdd, q_old[v], q_in[v], qu[v], src[v]);
+            }
+            break;
+        case kRk2Final:
+#pragma unroll
+            for (int v = 0; v < N; ++v) {
+                out[v] = combine(kRk2Final, q_old[v], q_in[v], qu[v], src[v]);
+            }
+            break;
+        case kSsp3Second:
+#pragma unroll
+            for (int v = 0; v < N; ++v) {
+                out[v] = combine(kSsp3Second, q_old[v], q_in[v], qu[v], src[v]);
+            }
+            break;
+        case kSsp3Final:
+#pragma unroll
+            for (int v = 0; v < N; ++v) {
+                out[v] = combine(kSsp3Final, q_old[v], q_in[v], qu[v], src[v]);
+            }
+            break;
+        case kHalfAdd:
+#pragma unroll
+            for (int v = 0; v < N; ++v) {
+                out[v] = combine(kHalfAdd, q_old[v], q_in[v], qu[v], src[v]);
+            }
+            break;
+        default:
+#pragma unroll
+            for (int v = 0; v < N; ++v) {
+                out[v] = combine(kSsp4Third, q_old[v], q_in[v], qu[v], src[v]);
+            }
+            break;
     }
 }
 

@@ -72,11 +72,14 @@ cudaError_t launch_one(const StageParams& p, int pass, cudaStream_t s) {
         }
         k<<<dim3(cdiv(p.nx, kTile), cdiv(p.ny, kTile), p.nz), dim3(kThreads), sm, s>>>(p);
     } else {
-        const dim3 g(cdiv(p.nx, kZBlockX), cdiv(p.ny, kZBlockY), cdiv(p.nz, kZChunk)), b(kZBlockX, kZBlockY);
-        if (p.ntracer > 0) {
-            zsweep3d_kernel<REC, LIM, RS, Real, MC_SRC, kMaxVars - 5><<<g, b, 0, s>>>(p);
-        } else {
-            zsweep3d_kernel<REC, LIM, RS, Real, MC_SRC, 0><<<g, b, 0, s>>>(p);
+        auto k = ztile3d_kernel<REC, LIM, RS, Real, MC_SRC>;
+        const size_t sm = ztile_smem_bytes<REC, Real>(p.nvar);
+        cudaError_t e = allow_smem(k, sm);
+        if (e == cudaSuccess) {
+            k<<<dim3(cdiv(p.nz, kTile), cdiv(p.nx, kZCols), p.ny), dim3(kThreads), sm, s>>>(p);
+        }
+        if (e != cudaSuccess) {
+            return e;
         }
     }
 #endif

@@ -23,9 +23,9 @@
 //     new state, scatters the ghost cells it is the source of, and (last
 //     stage) reduces the CFL minimum and status flags.
 // 3D splits each stage in two launches: the x-y plane pass above writes the
-// x+y divergence per cell, then a z-march kernel (one thread per (x, y)
-// column, a register window along z) adds the z divergence and finishes
-// the stage.
+// x+y divergence per cell, then a z pass (tiles of x columns by z cells,
+// one warp-wide sweep per column) adds the z divergence and finishes the
+// stage.
 #pragma once
 
 #include "common.cuh"
@@ -126,24 +126,44 @@ __device__ __forceinline__ double write_cell(const StageParams& p, int i, int j,
     if constexpr (NDIM > 2) {
         cz = axis_targets(k, p.nz, p.ng, p.bc.kind[4], p.bc.kind[5], iz, fz);
     }
-    for (int a = 0; a < cx; ++a) {
-        double qa[kMaxVars];
-#pragma unroll
-        for (int v = 0; v < kMaxVars; ++v) {
-            qa[v] = qn[v];
-        }
-        if (fx[a] >= 0) {
-            bc_transform<NDIM>(p.bc, 0, fx[a], nvar, qa);
-        }
-        for (int b = 0; b < cy; ++b) {
-            double qb[kMaxVars];
+    if constexpr (NDIM < 3) {
+        for (int a = 0; a < cx; ++a) {
+            double qa[kMaxVars];
 #pragma unroll
             for (int v = 0; v < kMaxVars; ++v) {
-                qb[v] = qa[v];
+                qa[v] = qn[v];
             }
-            if (fy[b] >= 0) {
-                bc_transform<NDIM>(p.bc, 1, fy[b], nvar, qb);
+            if (fx[a] >= 0) {
+                bc_transform<NDIM>(p.bc, 0, fx[a], nvar, qa);
             }
+            for (int b = 0; b < cy; ++b) {
+                if (a == 0 && b == 0) {
+                    continue;
+                }
+                double qb[kMaxVars];
+#pragma unroll
+                for (int v = 0; v < kMaxVars; ++v) {
+                    qb[v] = qa[v];
+                }
+                if (fy[b] >= 0) {
+                    bc_transform<NDIM>(p.bc, 1, fy[b], nvar, qb);
+                }
+#pragma unroll
+                for (int v = 0; v < kMaxVars; ++v) {
+                    if (v < nvar) {
+                        p.q_out[qidx(p, v, k, iy[b], ix[a])] = qb[v];
+                    }
+                }
+                account(qb);
+            }
+        }
+        return dtmin;
+    }
+    // 3D: each ghost target starts again from the cell's new state and
+    // applies the face transforms of its axes in x, y, z order, as the
+    // sequential per-axis fill does; only two states are live at a time
+    for (int a = 0; a < cx; ++a) {
+        for (int b = 0; b < cy; ++b) {
             for (int c = 0; c < cz; ++c) {
                 if (a == 0 && b == 0 && c == 0) {
                     continue;
@@ -151,7 +171,13 @@ __device__ __forceinline__ double write_cell(const StageParams& p, int i, int j,
                 double qc[kMaxVars];
 #pragma unroll
                 for (int v = 0; v < kMaxVars; ++v) {
-                    qc[v] = qb[v];
+                    qc[v] = qn[v];
+                }
+                if (fx[a] >= 0) {
+                    bc_transform<NDIM>(p.bc, 0, fx[a], nvar, qc);
+                }
+                if (fy[b] >= 0) {
+                    bc_transform<NDIM>(p.bc, 1, fy[b], nvar, qc);
                 }
                 if (fz[c] >= 0) {
                     bc_transform<NDIM>(p.bc, 2, fz[c], nvar, qc);
@@ -263,6 +289,58 @@ __device__ __forceinline__ void face_sweep(const T* centre, int stride, int vstr
     }
 }
 
+// load_prim split in two, for callers that issue the loads of several cells
+// before converting any: the hydro state of one cell (a benign state when
+// outside the array), then its primitives and tracer mass fractions stored
+// into shared memory.
+template <int NDIM>
+__device__ __forceinline__ void fetch_cons(const StageParams& p, int k, int j, int i, bool inb, double* q) {
+    constexpr int nh = 2 + NDIM;
+    if (inb) {
+        const double* src = p.q_in + qidx(p, 0, k, j, i);
+        const long long vs = (long long)p.zc * p.yc * p.xc;
+#pragma unroll
+        for (int v = 0; v < nh; ++v) {
+            q[v] = src[v * vs];
+        }
+    } else {
+        q[0] = 1.0;
+#pragma unroll
+        for (int v = 1; v < nh - 1; ++v) {
+            q[v] = 0.0;
+        }
+        q[nh - 1] = 1.0;
+    }
+}
+
+template <int NDIM, class T>
+__device__ __forceinline__ unsigned store_prim(const StageParams& p, int k, int j, int i, bool inb, const double* q,
+                                               T* w_smem, int var_stride) {
+    constexpr int nh = 2 + NDIM;
+    double w[nh];
+    prim_from_cons<NDIM>(p.gamma, q, w);
+#pragma unroll
+    for (int v = 0; v < nh; ++v) {
+        w_smem[v * var_stride] = T(w[v]);
+    }
+    if (p.ntracer > 0) {
+        const double inv_rho = 1.0 / q[0];
+        for (int t = 0; t < p.ntracer; ++t) {
+            const double qt = inb ? p.q_in[qidx(p, nh + t, k, j, i)] : 0.0;
+            w_smem[(nh + t) * var_stride] = T(qt * inv_rho);
+        }
+    }
+    if (!inb) {
+        return 0u;
+    }
+    bool fin = true;
+#pragma unroll
+    for (int v = 0; v < nh; ++v) {
+        fin = fin && isfinite(q[v]);
+    }
+    return state_flags(w[0], w[nh - 1], fin);
+}
+
 // ---------------------------------------------------------------------------
 // 1D: one warp updates one segment of kTile cells, independently of the
 // other warps of its CTA (so one CTA can serve segments of different
@@ -314,12 +392,16 @@ __device__ __forceinline__ void segment1d(const StageParams& p, int x0, T* W, do
             const long long id = qidx(p, v, 0, 0, i);
             qn[v] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, sdt[v]);
         }
-        for (int t = 0; t < p.ntracer; ++t) {
-            double qu = 0.0;
-            qu += double(d_tr[t]);
-            qu *= dtdx;
-            const long long id = qidx(p, nh + t, 0, 0, i);
-            qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0);
+        // constant tracer slots keep qn in registers
+#pragma unroll
+        for (int t = 0; t < kMaxVars - nh; ++t) {
+            if (t < p.ntracer) {
+                double qu = 0.0;
+                qu += double(d_tr[t]);
+                qu *= dtdx;
+                const long long id = qidx(p, nh + t, 0, 0, i);
+                qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0);
+            }
         }
         dtmin = smin(write_cell<NDIM>(p, i, 0, 0, qn, p.last != 0, &flags), dtmin);
     }
@@ -500,206 +582,166 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : k
 }
 
 // ---------------------------------------------------------------------------
-// 3D z pass: one thread per interior (x, y) column, marching along z over a
-// chunk of kZChunk cells with a register window of primitives. Adds the z
-// divergence to the x+y divergence from the plane pass and finishes the
-// stage. Passive tracers (up to kMaxVars - 5) in the NTR instantiation.
+// 3D z pass: adds the z divergence to the x+y divergence from the plane
+// pass and finishes the stage (passive tracers included).
 // ---------------------------------------------------------------------------
-constexpr int kZChunk = 32;
-constexpr int kZBlockX = 32, kZBlockY = 4;
+// Tile of the z pass: kZCols x-columns (one coalesced 256-byte row per
+// variable) by kTile z cells of one y row, with H halo rows above and below.
+constexpr int kZCols = 32;
 
-// The march is latency-bound. Each step loads the cell's own inputs of the
-// stage combination (x+y divergence, stage input, step-start state) before
-// the reconstruction and Riemann solve that precede their use, so those
-// loads overlap that arithmetic; with them, three CTAs of 128 threads per
-// SM (168 registers) measured 11 % faster on Sedov 512^3 than four CTAs
-// with the loads after the solve (128 registers, spilling). Loading the
-// next window cell one step ahead gained nothing.
-template <int REC, int LIM, int RS, class T, bool SRC = false, int NTR = 0>
-__global__ void __launch_bounds__(kZBlockX* kZBlockY, NTR > 0 ? 2 : 3) zsweep3d_kernel(StageParams p) {
+template <int REC>
+struct ZTileGeom {
+    static constexpr int H = halo_of<REC>();
+    static constexpr int TZ = kTile;
+    static constexpr int WZ = TZ + 2 * H;  // stored rows (z)
+    static constexpr int PZ = kZCols + 1;  // odd pitch: conflict-free z columns
+    static constexpr int WV = WZ * PZ;     // per-variable stride
+};
+
+template <int REC, class T>
+__host__ __device__ constexpr size_t ztile_smem_bytes(int nvar) {
+    return sizeof(T) * (size_t)nvar * ZTileGeom<REC>::WV;
+}
+
+// z pass: each CTA loads the primitives of its tile, sweeps every column
+// along z with one warp (lane L reconstructs cell L-1 of the column, solves
+// the face below it, and takes the next face's flux from lane L+1, exactly
+// like the x-y sweeps), overwrites the column with its z divergence -- no
+// other warp reads that column -- and then finishes each cell in row order
+// (coalesced): q_update = dq_xy + dFz as the x, y, z flux sum of
+// integrate_flux (source/TimeStepping.cpp:22-27), the stage combination, the
+// store and the ghost scatter. Grid: (z chunks, x tiles, y rows), z chunks
+// fastest, so the halo rows a neighbouring chunk re-reads are still in L2.
+template <int REC, int LIM, int RS, class T, bool SRC = false>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : kMinBlocks2d)
+    ztile3d_kernel(StageParams p) {
     if (p.dt_dev && p.blk->done) {
         return;
     }
     maybe_reset_min(p);
     constexpr int NDIM = 3;
     constexpr int nh = 5;
-    constexpr int S = stencil_half<REC>();
-    constexpr int WN = 2 * S + 1;  // window length
-    constexpr int TS = NTR > 0 ? NTR : 1;  // tracer slots compiled in (p.ntracer <= NTR used)
+    using G = ZTileGeom<REC>;
+    constexpr int H = G::H, TZ = G::TZ, WZ = G::WZ, PZ = G::PZ, WV = G::WV;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red_d[kWarps];
     __shared__ unsigned red_u[kWarps];
-    const int xi = blockIdx.x * kZBlockX + threadIdx.x;
-    const int yi = blockIdx.y * kZBlockY + threadIdx.y;
-    const int z0 = blockIdx.z * kZChunk;
-    const int z1 = min(z0 + kZChunk, p.nz);
-    const bool active = xi < p.nx && yi < p.ny;
-    const int i = xi + p.ng, j = yi + p.ng;
-    const T gamma = T(p.gamma);
-    const T gfac = T((p.gamma + 1.0) / (2.0 * p.gamma));
-    const double dt = stage_dt(p);
-    const double dtdx = dt / p.dx;
-    const long long cells = (long long)p.nx * p.ny * p.nz;
-    const int ntr = NTR > 0 ? p.ntracer : 0;
+    T* W = reinterpret_cast<T*>(smem_raw);
+
+    const int z0 = blockIdx.x * TZ;
+    const int x0 = blockIdx.y * kZCols;
+    const int yi = blockIdx.z;
+    const int j = p.ng + yi;
+    const int vw = min(kZCols, p.nx - x0);
+    const int vh = min(TZ, p.nz - z0);
     unsigned flags = 0;
     double dtmin = __longlong_as_double(0x7ff0000000000000ll);
 
-    if (active) {
-        // window[o][v] holds the primitives of cell (zc - S + o) where zc is
-        // the cell being reconstructed; wt[o][t] its tracers scaled to mass
-        // fractions (source/Hydro.cpp:27-33)
-        T win[WN][nh];
-        T wt[WN][TS];
-        auto load_w = [&](int zc_interior, int slot) {
-            double q[nh], wd[nh];
-            const int kk = zc_interior + p.ng;
+    // phase 1: primitives of the tile and its halo rows; every load of this
+    // thread's cells is issued before the first conversion
+    {
+        constexpr int items = WZ * kZCols;
+        constexpr int per = (items + kThreads - 1) / kThreads;
+        double q[per][nh];
 #pragma unroll
-            for (int v = 0; v < nh; ++v) {
-                q[v] = p.q_in[qidx(p, v, kk, j, i)];
-            }
-            prim_from_cons<NDIM>(p.gamma, q, wd);
-            bool fin = true;
-#pragma unroll
-            for (int v = 0; v < nh; ++v) {
-                fin = fin && isfinite(q[v]);
-                win[slot][v] = T(wd[v]);
-            }
-            if constexpr (NTR > 0) {
-                const double inv_rho = 1.0 / q[0];
-#pragma unroll
-                for (int t = 0; t < NTR; ++t) {
-                    wt[slot][t] = t < ntr ? T(p.q_in[qidx(p, nh + t, kk, j, i)] * inv_rho) : T(0);
-                }
-            }
-            return state_flags(wd[0], wd[nh - 1], fin);
-        };
-        // cells z0-1-S .. z0-1+S for the reconstruction of cell z0-1
-#pragma unroll
-        for (int o = 0; o < WN; ++o) {
-            flags |= load_w(z0 - 1 - S + o, o);
+        for (int u = 0; u < per; ++u) {
+            const int it = threadIdx.x + u * kThreads;
+            const int r = it / kZCols;
+            const int x = it - r * kZCols;
+            const int k = p.ng + z0 - H + r;
+            const bool inb = it < items && x < vw && k >= 0 && k < p.zc;
+            fetch_cons<NDIM>(p, k, j, p.ng + x0 + x, inb, q[u]);
         }
-        auto recon_window = [&](T* rl, T* rr, T* tl, T* tr) {
+#pragma unroll
+        for (int u = 0; u < per; ++u) {
+            const int it = threadIdx.x + u * kThreads;
+            if (it < items) {
+                const int r = it / kZCols;
+                const int x = it - r * kZCols;
+                const int k = p.ng + z0 - H + r;
+                const bool inb = x < vw && k >= 0 && k < p.zc;
+                flags |= store_prim<NDIM, T>(p, k, j, p.ng + x0 + x, inb, q[u], W + r * PZ + x, WV);
+            }
+        }
+    }
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const T gamma = T(p.gamma);
+    const T gfac = T((p.gamma + 1.0) / (2.0 * p.gamma));
+    const int ntr = p.ntracer;
+    const int c = lane - 1;  // this lane's cell along the column
+
+    // phase 2: z sweeps, one warp per column; the divergence replaces the
+    // column's primitives once every lane has read its stencil
+#pragma unroll 1
+    for (int col = warp; col < vw; col += kWarps) {
+        T* centre = W + (c + H) * PZ + col;
+        T d[nh], d_tr[kMaxVars];
+        face_sweep<NDIM, REC, LIM, RS, T>(centre, PZ, WV, ntr, gamma, gfac, 2, d, d_tr);
+        __syncwarp();
+        if (lane >= 1 && lane <= TZ) {
 #pragma unroll
             for (int v = 0; v < nh; ++v) {
-                T s[5];
-#pragma unroll
-                for (int o = 0; o < WN; ++o) {
-                    s[2 - S + o] = win[o][v];
-                }
-                reconstruct<REC, LIM>(s, rl[v], rr[v]);
+                centre[v * WV] = d[v];
             }
-            if constexpr (NTR > 0) {
-#pragma unroll
-                for (int t = 0; t < NTR; ++t) {
-                    T s[5];
-#pragma unroll
-                    for (int o = 0; o < WN; ++o) {
-                        s[2 - S + o] = wt[o][t];
-                    }
-                    reconstruct<REC, LIM>(s, tl[t], tr[t]);
-                }
+            for (int t = 0; t < ntr; ++t) {
+                centre[(nh + t) * WV] = d_tr[t];
             }
-        };
-        auto shift_in = [&](int zc_interior) {
-#pragma unroll
-            for (int o = 0; o < WN - 1; ++o) {
-#pragma unroll
-                for (int v = 0; v < nh; ++v) {
-                    win[o][v] = win[o + 1][v];
-                }
-                if constexpr (NTR > 0) {
-#pragma unroll
-                    for (int t = 0; t < NTR; ++t) {
-                        wt[o][t] = wt[o + 1][t];
-                    }
-                }
-            }
-            flags |= load_w(zc_interior, WN - 1);
-        };
-        // tracer flux of a face: upwinded by the sign of the mass flux
-        // (source/Hydro.cpp:155-162)
-        auto tracer_flux = [&](const T* f, const T* tleft, const T* tright, T* ft) {
-            if constexpr (NTR > 0) {
-#pragma unroll
-                for (int t = 0; t < NTR; ++t) {
-                    ft[t] = (f[0] >= T(0)) ? f[0] * tleft[t] : f[0] * tright[t];
-                }
-            }
-        };
-        T rr_prev[nh], rl_cur[nh], rr_cur[nh], f_prev[nh], f_cur[nh];
-        T tr_prev[TS], tl_cur[TS], tr_cur[TS], ft_prev[TS], ft_cur[TS];
-        {
-            T rl_tmp[nh], tl_tmp[TS];
-            recon_window(rl_tmp, rr_prev, tl_tmp, tr_prev);  // cell z0-1
         }
-        shift_in(z0 + S);
-        recon_window(rl_cur, rr_cur, tl_cur, tr_cur);  // cell z0
-        riemann<RS, NDIM>(gamma, gfac, 2, rr_prev, rl_cur, f_prev);  // face z0 - 1/2
-        tracer_flux(f_prev, tr_prev, tl_cur, ft_prev);
+    }
+    __syncthreads();
+
+    // phase 3: finish every cell of the tile, x fastest
+    const double dt = stage_dt(p);
+    const double dtdx = dt / p.dx;
+    const bool old = combo_reads_old(p.combo);
+    const long long cells = (long long)p.nx * p.ny * p.nz;
+    const long long vs = (long long)p.zc * p.yc * p.xc;  // variable stride of the state
+#pragma unroll 1
+    for (int it = threadIdx.x; it < TZ * kZCols; it += kThreads) {
+        const int zr = it / kZCols;
+        const int x = it - zr * kZCols;
+        if (x >= vw || zr >= vh) {
+            continue;
+        }
+        const int i = p.ng + x0 + x;
+        const int kk = p.ng + z0 + zr;
+        const long long o = ((long long)(z0 + zr) * p.ny + yi) * p.nx + (x0 + x);
+        const long long id0 = qidx(p, 0, kk, j, i);
+        const T* dz = W + (zr + H) * PZ + x;
+        double qo[nh], qi[nh], qu[nh], sdt[nh];
 #pragma unroll
         for (int v = 0; v < nh; ++v) {
-            rr_prev[v] = rr_cur[v];
+            qu[v] = p.dqxy[v * cells + o];
+            qi[v] = p.q_in[id0 + v * vs];
+            qo[v] = old ? p.q_old[id0 + v * vs] : 0.0;
         }
+        source_dt_of<NDIM, SRC>(p, qi, dt, sdt);
 #pragma unroll
-        for (int t = 0; t < TS; ++t) {
-            tr_prev[t] = tr_cur[t];
+        for (int v = 0; v < nh; ++v) {
+            qu[v] += double(dz[v * WV]);
+            qu[v] *= dtdx;
         }
-        const bool old = combo_reads_old(p.combo);
-        for (int z = z0; z < z1; ++z) {
-            const int kk = z + p.ng;
-            const long long o = ((long long)z * p.ny + yi) * p.nx + xi;
-            // the cell's own inputs of the stage combination are loaded
-            // before its reconstruction and Riemann solve, so their memory
-            // latency overlaps that arithmetic
-            double dq[nh], qi[nh], qo[nh];
+        double qn[kMaxVars];
 #pragma unroll
-            for (int v = 0; v < nh; ++v) {
-                const long long id = qidx(p, v, kk, j, i);
-                dq[v] = p.dqxy[v * cells + o];
-                qi[v] = p.q_in[id];
-                qo[v] = old ? p.q_old[id] : 0.0;
-            }
-            shift_in(z + 1 + S);
-            recon_window(rl_cur, rr_cur, tl_cur, tr_cur);  // cell z+1
-            riemann<RS, NDIM>(gamma, gfac, 2, rr_prev, rl_cur, f_cur);  // face z + 1/2
-            tracer_flux(f_cur, tr_prev, tl_cur, ft_cur);
-            double qn[kMaxVars];
+        for (int v = nh; v < kMaxVars; ++v) {
+            qn[v] = 0.0;
+        }
+        combine_all<nh>(p.combo, qo, qi, qu, sdt, qn);
+        // constant tracer slots keep qn in registers
 #pragma unroll
-            for (int v = 0; v < kMaxVars; ++v) {
-                qn[v] = 0.0;
-            }
-            double sdt[nh];
-            source_dt<NDIM, SRC>(p, kk, j, i, dt, sdt);
-#pragma unroll
-            for (int v = 0; v < nh; ++v) {
-                double qu = dq[v];
-                qu += double(f_prev[v] - f_cur[v]);
-                qu *= dtdx;
-                qn[v] = combine(p.combo, qo[v], qi[v], qu, sdt[v]);
-            }
-            if constexpr (NTR > 0) {
-#pragma unroll
-                for (int t = 0; t < NTR; ++t) {
-                    if (t < ntr) {
-                        double qu = p.dqxy[(nh + t) * cells + o];
-                        qu += double(ft_prev[t] - ft_cur[t]);
-                        qu *= dtdx;
-                        const long long id = qidx(p, nh + t, kk, j, i);
-                        qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0);
-                    }
-                }
-            }
-            dtmin = smin(write_cell<NDIM>(p, i, j, kk, qn, p.last != 0, &flags), dtmin);
-#pragma unroll
-            for (int v = 0; v < nh; ++v) {
-                f_prev[v] = f_cur[v];
-                rr_prev[v] = rr_cur[v];
-            }
-#pragma unroll
-            for (int t = 0; t < TS; ++t) {
-                ft_prev[t] = ft_cur[t];
-                tr_prev[t] = tr_cur[t];
+        for (int t = 0; t < kMaxVars - nh; ++t) {
+            if (t < ntr) {
+                double qt = p.dqxy[(nh + t) * cells + o];
+                qt += double(dz[(nh + t) * WV]);
+                qt *= dtdx;
+                const long long id = id0 + (nh + t) * vs;
+                qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qt, 0.0);
             }
         }
+        dtmin = smin(write_cell<NDIM>(p, i, j, kk, qn, p.last != 0, &flags), dtmin);
     }
     block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
 }
