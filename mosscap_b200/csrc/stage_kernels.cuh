@@ -98,10 +98,14 @@ __device__ __forceinline__ double write_cell(const StageParams& p, int i, int j,
             dtmin = smin(d, dtmin);
         }
     };
+    const long long vs = (long long)p.zc * p.yc * p.xc;  // variable stride of the state
+    {
+        double* dst = p.q_out + qidx(p, 0, k, j, i);
 #pragma unroll
-    for (int v = 0; v < kMaxVars; ++v) {
-        if (v < nvar) {
-            p.q_out[qidx(p, v, k, j, i)] = qn[v];
+        for (int v = 0; v < kMaxVars; ++v) {
+            if (v < nvar) {
+                dst[v * vs] = qn[v];
+            }
         }
     }
     account(qn);
@@ -202,10 +206,12 @@ __device__ __forceinline__ unsigned load_prim(const StageParams& p, int k, int j
                                               int var_stride) {
     constexpr int nh = 2 + NDIM;
     double q[nh], w[nh];
+    const long long vs = (long long)p.zc * p.yc * p.xc;  // variable stride of the state
+    const long long id0 = qidx(p, 0, k, j, i);
     if (inb) {
 #pragma unroll
         for (int v = 0; v < nh; ++v) {
-            q[v] = p.q_in[qidx(p, v, k, j, i)];
+            q[v] = p.q_in[id0 + v * vs];
         }
     } else {
         // outside the array: a benign state that no stored result depends on
@@ -224,7 +230,7 @@ __device__ __forceinline__ unsigned load_prim(const StageParams& p, int k, int j
     if (p.ntracer > 0) {
         const double inv_rho = 1.0 / q[0];
         for (int t = 0; t < p.ntracer; ++t) {
-            const double qt = inb ? p.q_in[qidx(p, nh + t, k, j, i)] : 0.0;
+            const double qt = inb ? p.q_in[id0 + (nh + t) * vs] : 0.0;
             w_smem[(nh + t) * var_stride] = T(qt * inv_rho);
         }
     }
@@ -538,24 +544,30 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
                 for (int v = 0; v < kMaxVars; ++v) {
                     qn[v] = 0.0;
                 }
-                double sdt[nh];
-                source_dt<NDIM, SRC>(p, 0, j, i, dt, sdt);
+                const long long vs = (long long)p.zc * p.yc * p.xc;  // variable stride of the state
+                const long long id0 = qidx(p, 0, 0, j, i);
+                double qo[nh], qi[nh], qu[nh], sdt[nh];
 #pragma unroll
                 for (int v = 0; v < nh; ++v) {
-                    double qu = 0.0;
-                    qu += double(d[v]);
-                    qu += double(dfy[v * YV]);
-                    qu *= dtdx;
-                    const long long id = qidx(p, v, 0, j, i);
-                    qn[v] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, sdt[v]);
+                    qi[v] = p.q_in[id0 + v * vs];
+                    qo[v] = old ? p.q_old[id0 + v * vs] : 0.0;
                 }
+                source_dt_of<NDIM, SRC>(p, qi, dt, sdt);
+#pragma unroll
+                for (int v = 0; v < nh; ++v) {
+                    qu[v] = 0.0;
+                    qu[v] += double(d[v]);
+                    qu[v] += double(dfy[v * YV]);
+                    qu[v] *= dtdx;
+                }
+                combine_all<nh>(p.combo, qo, qi, qu, sdt, qn);
                 for (int t = 0; t < ntr; ++t) {
-                    double qu = 0.0;
-                    qu += double(d_tr[t]);
-                    qu += double(dfy[(nh + t) * YV]);
-                    qu *= dtdx;
-                    const long long id = qidx(p, nh + t, 0, j, i);
-                    qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0);
+                    double qt = 0.0;
+                    qt += double(d_tr[t]);
+                    qt += double(dfy[(nh + t) * YV]);
+                    qt *= dtdx;
+                    const long long id = id0 + (nh + t) * vs;
+                    qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qt, 0.0);
                 }
                 dtmin = smin(write_cell<NDIM>(p, i, j, 0, qn, p.last != 0, &flags), dtmin);
             }
