@@ -249,7 +249,8 @@ __device__ __forceinline__ unsigned load_prim(const StageParams& p, int k, int j
 // 2D WENO5-Z sweep is instruction-fetch bound when its four
 // reconstructions are unrolled (instruction-cache hit rate 63 %); two per
 // iteration measured 5 % faster on KH 2048^2 than four, and one per
-// iteration 3 %. Everything else is fully unrolled.
+// iteration 3 %. Everything else is fully unrolled (one PPM reconstruction
+// per iteration made the 3D plane pass 4 % slower).
 template <int NDIM, int REC>
 __host__ __device__ constexpr int recon_group() {
     return (REC == kWeno5z && NDIM == 2) ? 2 : 2 + NDIM;
