@@ -70,7 +70,7 @@ cudaError_t launch_one(const StageParams& p, int pass, cudaStream_t s) {
         if (e != cudaSuccess) {
             return e;
         }
-        k<<<dim3(cdiv(p.nx, kTile), cdiv(p.ny, kTile), p.nz), dim3(kThreads), sm, s>>>(p);
+        k<<<dim3(cdiv(p.nx, kTile), cdiv(p.ny, kTile), p.nz), dim3(tile_threads<3, Real>()), sm, s>>>(p);
     } else {
         auto k = ztile3d_kernel<REC, LIM, RS, Real, MC_SRC>;
         const size_t sm = ztile_smem_bytes<REC, Real>(p.nvar);

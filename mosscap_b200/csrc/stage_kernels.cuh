@@ -435,10 +435,11 @@ __global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
 // One CTA updates tile (bx, by) of a 2D problem, or of z plane bz in the 3D
 // plane pass. smem holds nvar x (WY x P) primitives and nvar x (TY x PY)
 // y divergences. Contains CTA-wide barriers: every thread of the CTA calls it.
-template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false>
+template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false, int NT = kThreads>
 __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int bz, T* smem, double& dtmin,
                                        unsigned& flags) {
     constexpr int nh = 2 + NDIM;
+    constexpr int NW = NT / 32;
     using G = TileGeom<2, REC>;
     constexpr int H = G::H, TX = G::TX, TY = G::TY, WX = G::WX, P = G::P, WY = G::WY, PY = G::PY;
     constexpr int WV = WY * P;   // per-variable stride of W
@@ -455,7 +456,7 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
     // phase 1: primitives of the tile and its cross-shaped halo
     constexpr int core = TY * WX;
     constexpr int items = core + 2 * H * TX;
-    for (int it = threadIdx.x; it < items; it += kThreads) {
+    for (int it = threadIdx.x; it < items; it += NT) {
         int tx, ty;
         if (it < core) {
             ty = it / WX;
@@ -492,7 +493,7 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
     for (int pass = 0; pass < 2; ++pass) {
         const int axis = 1 - pass;
         const int nlines = axis == 1 ? vw : vh;
-        for (int line = warp; line < nlines; line += kWarps) {
+        for (int line = warp; line < nlines; line += NW) {
             const T* centre = axis == 0 ? W + (line + H) * P + (c + H) : W + (c + H) * P + (line + H);
             T d[nh], d_tr[kMaxVars];
             face_sweep<NDIM, REC, LIM, RS, T>(centre, axis == 0 ? 1 : P, WV, ntr, gamma, gfac, axis, d, d_tr);
@@ -570,19 +571,33 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
     }
 }
 
+// Threads per CTA of the tiled stage kernel and CTAs per SM it is compiled
+// for. The 3D FP64 plane pass holds five variables' tiles (90 KB of shared
+// memory), so two CTAs fit per SM; it runs 384 threads per CTA to keep 24
+// warps resident at the same 80 registers.
+template <int NDIM, class T>
+__host__ __device__ constexpr int tile_threads() {
+    return (NDIM == 3 && sizeof(T) == 8) ? 384 : kThreads;
+}
+template <int NDIM, class T>
+__host__ __device__ constexpr int tile_min_blocks() {
+    return sizeof(T) == 4 ? kMinBlocks2dF32 : (NDIM == 3 ? 2 : kMinBlocks2d);
+}
+
 template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : kMinBlocks2d)
+__global__ void __launch_bounds__(tile_threads<NDIM, T>(), tile_min_blocks<NDIM, T>())
     stage2d_kernel(StageParams p) {
     if (p.dt_dev && p.blk->done) {
         return;
     }
     maybe_reset_min(p);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red_d[kWarps];
-    __shared__ unsigned red_u[kWarps];
+    constexpr int NT = tile_threads<NDIM, T>();
+    __shared__ double red_d[NT / 32];
+    __shared__ unsigned red_u[NT / 32];
     double dtmin = __longlong_as_double(0x7ff0000000000000ll);
     unsigned flags = 0;
-    tile2d<NDIM, REC, LIM, RS, T, SRC>(p, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<T*>(smem_raw), dtmin,
+    tile2d<NDIM, REC, LIM, RS, T, SRC, NT>(p, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<T*>(smem_raw), dtmin,
                                   flags);
     block_publish(dtmin, flags, NDIM != 3 && p.last != 0, p.blk, red_d, red_u);
 }
