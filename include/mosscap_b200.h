@@ -205,6 +205,15 @@ mc_status mc_update_eos(mc_ctx* ctx, double* Q, void* stream);
  * host memory; either may be NULL). */
 mc_status mc_get_eos_fields(mc_ctx* ctx, double* y, double* T, void* stream);
 
+/* Fills W (device memory, the layout of Q) with the primitive state the
+ * reference's State.W holds after its last time_step: global_cons_to_prim
+ * (source/Hydro.cpp:8-53) of the input of the step's last stage, over every
+ * cell, ghosts included, tracers as mass fractions. The library keeps that
+ * stage input in its own stage buffer. Before the context's first step, Q
+ * (the caller's state) is converted instead. What write_output stores as
+ * "W" (source/Output.cpp:226-229). */
+mc_status mc_get_prim(mc_ctx* ctx, const double* Q, double* W, void* stream);
+
 /* Registers the gravity source term (setup_gravity,
  * source/SourceTerms/Gravity.cpp:44-70; config keys sources.gravity.x/y/z):
  * every stage adds dt * (0, rho g_x, rho g_y, rho g_z, m . g) to the hydro

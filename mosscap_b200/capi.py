@@ -159,6 +159,8 @@ def load() -> ctypes.CDLL:
     lib.mc_update_eos.restype = i32
     lib.mc_get_eos_fields.argtypes = [vp, vp, vp, vp]
     lib.mc_get_eos_fields.restype = i32
+    lib.mc_get_prim.argtypes = [vp, vp, vp, vp]
+    lib.mc_get_prim.restype = i32
     lib.mc_launch_count.argtypes = [vp]
     lib.mc_launch_count.restype = i64
     lib.mc_adjoint_create.argtypes = [P(McGrid), P(McScheme), i32, P(vp)]

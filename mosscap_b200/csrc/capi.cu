@@ -50,6 +50,7 @@ struct mc_ctx {
     double tab_x0 = 0.0, tab_dx = 1.0, tab_y0 = 0.0, tab_dy = 1.0;
     int tab_nx = 0, tab_ny = 0;
     double* buf_eos = nullptr;    // tabulated: the first stage's shifted input
+    const double* last_stage_in = nullptr;  // input of the last stage of the latest step
     // kernel timing (mc_profile_stages)
     bool profiling = false;
     struct Timed {
@@ -215,6 +216,7 @@ mc::EosLaunch eos_launch(const mc_ctx* c, const double* q_in, double* q_out, boo
 mc_status enqueue_step(mc_ctx* c, double* Q, double dt, const double* dt_dev, bool reset_min, cudaStream_t s) {
     const StagePlan plan = plan_for(c->scheme.time_stepper);
     double* bufs[3] = {Q, c->buf_a, c->buf_b};
+    c->last_stage_in = bufs[plan.in[plan.n - 1]];
     for (int st = 0; st < plan.n; ++st) {
         StageParams p = base_params(c);
         p.q_in = bufs[plan.in[st]];
@@ -534,6 +536,21 @@ mc_status mc_get_eos_fields(mc_ctx* c, double* y, double* T, void* stream) {
     if (T) {
         MC_CUDA(cudaMemcpyAsync(T, c->eos_T, bytes, cudaMemcpyDefault, s), "EOS fields");
     }
+    return MC_OK;
+}
+
+mc_status mc_get_prim(mc_ctx* c, const double* Q, double* W, void* stream) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    const double* src = c->last_stage_in ? c->last_stage_in : Q;
+    if (!W || !src) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null W, or null Q before the first step");
+    }
+    StageParams p = base_params(c);
+    p.q_in = src;
+    c->launches += 1;
+    MC_CUDA(mc::launch_cons_to_prim(p, W, c->grid.num_dim, (cudaStream_t)stream), "cons_to_prim launch");
     return MC_OK;
 }
 

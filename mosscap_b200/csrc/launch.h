@@ -25,6 +25,9 @@ cudaError_t launch_stage_d3_fp32_src(const StageParams& p, int rec, int lim, int
 
 // Ghost fill of Q from its interior (every built-in boundary kind).
 cudaError_t launch_fill_bcs(const StageParams& p, int ndim, cudaStream_t s);
+// Primitives of p.q_in over every cell (ghosts included) into w, tracers
+// as mass fractions.
+cudaError_t launch_cons_to_prim(const StageParams& p, double* w, int ndim, cudaStream_t s);
 // CFL minimum over every cell of Q (ghosts included) into blk->cfl_min_bits,
 // which the launch first resets.
 cudaError_t launch_cfl_min(const StageParams& p, int ndim, cudaStream_t s);

@@ -89,7 +89,49 @@ __global__ void clock_advance_kernel(DeviceBlock* blk, double* dt_log, int first
     advance_clock(blk, dt_log, first != 0, true);
 }
 
+// global_cons_to_prim (source/Hydro.cpp:8-53) over every cell, ghosts
+// included: the hydro primitives of q_in, and each tracer times 1 / rho.
+template <int NDIM>
+__global__ void __launch_bounds__(256) cons_to_prim_kernel(StageParams p, double* w_out) {
+    constexpr int nh = 2 + NDIM;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < p.plane;
+         c += (long long)gridDim.x * blockDim.x) {
+        double q[nh], w[nh];
+#pragma unroll
+        for (int v = 0; v < nh; ++v) {
+            q[v] = p.q_in[v * p.plane + c];
+        }
+        prim_from_cons<NDIM>(p.gamma, q, w);
+#pragma unroll
+        for (int v = 0; v < nh; ++v) {
+            w_out[v * p.plane + c] = w[v];
+        }
+        if (p.ntracer > 0) {
+            const double inv_rho = 1.0 / q[0];
+            for (int t = 0; t < p.ntracer; ++t) {
+                w_out[(nh + t) * p.plane + c] = p.q_in[(nh + t) * p.plane + c] * inv_rho;
+            }
+        }
+    }
+}
+
 } // namespace
+
+cudaError_t launch_cons_to_prim(const StageParams& p, double* w, int ndim, cudaStream_t s) {
+    const int blocks = (int)(p.plane < 148LL * 8 * 256 ? cdiv(p.plane, 256) : 148 * 8);
+    switch (ndim) {
+        case 1:
+            cons_to_prim_kernel<1><<<blocks, 256, 0, s>>>(p, w);
+            break;
+        case 2:
+            cons_to_prim_kernel<2><<<blocks, 256, 0, s>>>(p, w);
+            break;
+        default:
+            cons_to_prim_kernel<3><<<blocks, 256, 0, s>>>(p, w);
+            break;
+    }
+    return cudaGetLastError();
+}
 
 cudaError_t launch_fill_bcs(const StageParams& p, int ndim, cudaStream_t s) {
     const long long n = (long long)p.nx * p.ny * p.nz;

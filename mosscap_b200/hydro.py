@@ -159,6 +159,17 @@ class HydroSim:
         torch.cuda.synchronize(self.device)
         return y.cpu().numpy(), T.cpu().numpy()
 
+    def get_W(self) -> np.ndarray:
+        """The primitive state the reference's State.W holds after its last
+        time_step (the last stage's input through global_cons_to_prim,
+        source/Hydro.cpp:8-53), ghosts included; before the first step, the
+        primitives of Q (mc_get_prim)."""
+        W = torch.empty_like(self.Q)
+        capi.check(self.lib.mc_get_prim(self.ctx, self._qptr(), ctypes.c_void_p(W.data_ptr()), self._stream()),
+                   "mc_get_prim")
+        torch.cuda.synchronize(self.device)
+        return W.cpu().numpy()
+
     def status(self) -> int:
         f = ctypes.c_uint32()
         capi.check(self.lib.mc_get_status(self.ctx, ctypes.byref(f), self._stream()), "mc_get_status")
@@ -193,13 +204,22 @@ class HydroSim:
         self.current_step += done.value
         return log[:done.value].copy()
 
-    def run(self, max_steps: int = 1 << 62, device_loop: bool = True) -> np.ndarray:
-        """The main loop of source/main.cpp:54-72 (outputs only move the clock)."""
+    def run(self, max_steps: int = 1 << 62, device_loop: bool = True, output=None) -> np.ndarray:
+        """The main loop of source/main.cpp:54-72. Without `output` (an
+        :class:`~mosscap_b200.output.OutputConfig`) outputs only move the
+        clock; with it, the files of source/Output.cpp are written: first the
+        initial output if none has been written yet (setup_sim,
+        source/SetupModules.hpp:259), then one after every step that makes
+        an output due, and a last one when the loop ends."""
+        from .output import write_output
+        if output is not None and output.prev_output_time < 0.0:
+            write_output(self, output)
         dts = []
         n = 0
         while self.time < self.max_time and n < max_steps:
             if device_loop:
-                d = self.advance(max_steps - n)
+                # the dt log of one call is host memory: bounded chunks
+                d = self.advance(min(max_steps - n, 1 << 16))
                 dts.extend(d.tolist())
                 n += len(d)
                 if len(d) == 0:
@@ -211,6 +231,10 @@ class HydroSim:
                 n += 1
                 if self.time >= self.prev_output_time + self.output_delta:
                     self.prev_output_time = self.time
+            if output is not None and self.time >= output.prev_output_time + self.output_delta:
+                write_output(self, output)
+        if output is not None:
+            write_output(self, output)
         return np.asarray(dts)
 
     def get_Q(self) -> np.ndarray:
