@@ -51,12 +51,19 @@ __host__ __device__ constexpr size_t batch_smem_bytes() {
 // registers than the single-problem kernel to keep them resident (two CTAs
 // with up to 128 registers measured 7 % faster than three with 80).
 constexpr int kMinBlocksBatch = 2;
+// Threads per CTA: the 2D tiles run 320 (ten warps, three of a pass's 30
+// lines each; 24 % faster than 256 on the 4096-problem set), the 1D bundles
+// one task per warp of 256.
+template <int PART>
+__host__ __device__ constexpr int batch_threads() {
+    return PART == kPart2d ? 320 : kThreads;
+}
 
 template <int REC, int LIM, int RS, class T, int PART>
-__global__ void __launch_bounds__(kThreads, kMinBlocksBatch) batch_stage_kernel(BatchStageParams bp) {
+__global__ void __launch_bounds__(batch_threads<PART>(), kMinBlocksBatch) batch_stage_kernel(BatchStageParams bp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red_d[kWarps];
-    __shared__ unsigned red_u[kWarps];
+    __shared__ double red_d[batch_threads<PART>() / 32];
+    __shared__ unsigned red_u[batch_threads<PART>() / 32];
     __shared__ int s_item;
     T* smem = reinterpret_cast<T*>(smem_raw);
     const int warp = threadIdx.x >> 5;
@@ -81,7 +88,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksBatch) batch_stage_kernel(
             if (!p.blk->done) {
                 double dtmin = __longlong_as_double((long long)kInfBits);
                 unsigned flags = 0;
-                tile2d<2, REC, LIM, RS, T>(p, it.bx, it.by, 0, smem, dtmin, flags);
+                tile2d<2, REC, LIM, RS, T, false, batch_threads<PART>()>(p, it.bx, it.by, 0, smem, dtmin, flags);
                 block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
             }
         } else {

@@ -26,9 +26,9 @@ cudaError_t launch_batch_part(const BatchStageParams& bp, int grid, cudaStream_t
         return e;
     }
     if (occupancy) {
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, k, kThreads, sm);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, k, batch_threads<PART>(), sm);
     }
-    k<<<grid, kThreads, sm, s>>>(bp);
+    k<<<grid, batch_threads<PART>(), sm, s>>>(bp);
     return cudaGetLastError();
 }
 

@@ -61,7 +61,7 @@ cudaError_t launch_one(const StageParams& p, int pass, cudaStream_t s) {
     if (e != cudaSuccess) {
         return e;
     }
-    k<<<dim3(cdiv(p.nx, kTile), cdiv(p.ny, kTile)), dim3(kThreads), sm, s>>>(p);
+    k<<<dim3(cdiv(p.nx, kTile), cdiv(p.ny, kTile)), dim3(tile_threads<2, Real>()), sm, s>>>(p);
 #else
     if (pass == 0) {
         auto k = stage2d_kernel<3, REC, LIM, RS, Real>;

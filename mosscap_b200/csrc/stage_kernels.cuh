@@ -33,12 +33,11 @@
 namespace mc {
 
 constexpr int kTile = 30;     // output cells per warp-wide row segment
-constexpr int kThreads = 256; // threads per CTA of the tiled kernels
+constexpr int kThreads = 256; // threads per CTA of the 1D and z-pass kernels (2D: tile_threads)
 constexpr int kWarps = kThreads / 32;
-// CTAs per SM the 2D / plane kernel is compiled for. FP64: three (80
-// registers a thread); with the x divergence kept in registers its shared
-// memory (72 KB for four variables) allows three. FP32 compute form: four
-// (64 registers; measured faster than three despite a few spills).
+// CTAs per SM of the 256-thread kernels: FP64 three (80 registers a
+// thread), FP32 four (64 registers; measured faster than three despite a
+// few spills).
 constexpr int kMinBlocks2d = 3;
 constexpr int kMinBlocks2dF32 = 4;
 
@@ -572,16 +571,23 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
 }
 
 // Threads per CTA of the tiled stage kernel and CTAs per SM it is compiled
-// for. The 3D FP64 plane pass holds five variables' tiles (90 KB of shared
-// memory), so two CTAs fit per SM; it runs 384 threads per CTA to keep 24
-// warps resident at the same 80 registers.
+// for. A sweep pass has 30 lines: with 10 warps every warp takes exactly
+// three (with 8, six warps take four and two take three).
+//   2D FP64: two CTAs of 320 threads per SM (20 warps, up to 96 registers,
+//     72 KB of shared memory each): 3 % faster on KH 2048^2 than three CTAs
+//     of 256 at 80 registers, 24 % faster in the batched form.
+//   2D FP32: three CTAs of 320 threads (64 registers, a few spilled): 3 %
+//     faster than four of 256.
+//   3D FP64 plane pass: five variables' tiles take 90 KB of shared memory,
+//     two CTAs per SM; 384 threads (24 warps at 80 registers) measured 2 %
+//     faster than 320 and 11 % faster than 256.
 template <int NDIM, class T>
 __host__ __device__ constexpr int tile_threads() {
-    return (NDIM == 3 && sizeof(T) == 8) ? 384 : kThreads;
+    return NDIM == 1 ? kThreads : ((NDIM == 3 && sizeof(T) == 8) ? 384 : 320);
 }
 template <int NDIM, class T>
 __host__ __device__ constexpr int tile_min_blocks() {
-    return sizeof(T) == 4 ? kMinBlocks2dF32 : (NDIM == 3 ? 2 : kMinBlocks2d);
+    return NDIM == 1 ? (sizeof(T) == 4 ? kMinBlocks2dF32 : kMinBlocks2d) : (sizeof(T) == 4 ? 3 : 2);
 }
 
 template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false>
