@@ -248,8 +248,9 @@ __device__ __forceinline__ unsigned load_prim(const StageParams& p, int k, int j
 // 2D WENO5-Z sweep is instruction-fetch bound when its four
 // reconstructions are unrolled (instruction-cache hit rate 63 %); two per
 // iteration measured 5 % faster on KH 2048^2 than four, and one per
-// iteration 3 %. Everything else is fully unrolled (one PPM reconstruction
-// per iteration made the 3D plane pass 4 % slower).
+// iteration 3 %; with 320-thread CTAs and 96 registers the unrolled form
+// is still 0.6 % slower. Everything else is fully unrolled (one PPM
+// reconstruction per iteration made the 3D plane pass 4 % slower).
 template <int NDIM, int REC>
 __host__ __device__ constexpr int recon_group() {
     return (REC == kWeno5z && NDIM == 2) ? 2 : 2 + NDIM;
