@@ -62,6 +62,9 @@ def parse():
                          "or an independent problem per GPU (replicas)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="kh2d at N=1: skip the FP32 form, Sedov 512^3, batch and adjoint measurements "
+                         "that the default run adds to the line under 'forms'")
     return ap.parse_args()
 
 
@@ -192,6 +195,22 @@ def cpu_run(n, steps, warmup, budget_s=None):
     return n * n * done / dt, done, dt, kind, cores
 
 
+def cpu_baseline_subprocess(n, budget_s):
+    """The CPU baseline timed in a process of its own (no CUDA context, no
+    clock sampler beside it), so that its OpenMP threads have the host cores
+    to themselves; returns the cpu_baseline object."""
+    code = ("import json, sys; sys.path.insert(0, %r); import bench; "
+            "v, done, secs, kind, cores = bench.cpu_run(%d, 1000, 1, budget_s=%r); "
+            "print(json.dumps([v, done, secs, kind, cores]))") % (ROOT, n, float(budget_s))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    if r.returncode != 0:
+        return {"error": r.stderr.strip().splitlines()[-1] if r.stderr.strip() else f"rc {r.returncode}"}
+    v, done, secs, kind, cores = json.loads(r.stdout.strip().splitlines()[-1])
+    return {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{done} full SSPRK3 steps of the {n}x{n} problem ({secs:.1f} s, {cores} threads, "
+                      f"in a CPU-only child process after the GPU work)"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -309,6 +328,12 @@ def run_ours(args):
                 "alg_bytes_per_launch": alg_bytes_per_launch, "avg_launch_ms": avg_launch_ms,
                 "launches_timed": stage_n}
 
+    # the density after warmup + K steps, for the FP32 form's error
+    rho64 = None
+    if rank == 0 and world == 1 and not args.no_extras and args.precision == "fp64":
+        ng = p.ng
+        rho64 = sim.Q[0, 0, ng:-ng, ng:-ng].clone()
+
     # ---- end to end through the C ABI with host buffers --------------------
     e2e = None
     if not args.no_e2e:
@@ -335,12 +360,16 @@ def run_ours(args):
                "how": "per step: pinned-host state -> device, mc_compute_dt (dt read back), mc_time_step, "
                       "state -> pinned host, synchronize"}
 
+    # ---- the other forms, measured in this run (rank 0, N = 1) ------------
+    extras = None
+    if rank == 0 and world == 1 and not args.no_extras and args.precision == "fp64":
+        extras = run_extras(args, rho64, value)
+        rho64 = None
+
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, done, secs, kind, cores = cpu_run(n, 1000, 1, budget_s=15.0)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
-               "sample": f"{done} full SSPRK3 steps of the {n}x{n} problem ({secs:.1f} s, {cores} threads)"}
+        cpu = cpu_baseline_subprocess(n, budget_s=15.0)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -349,91 +378,126 @@ def run_ours(args):
                 "data": "synthetic", "config": config(n, args.precision, world, args.decomp), "roofline": roofline,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
                 "status_flags": int(flags)}
+        if extras is not None:
+            line["forms"] = extras
         print(json.dumps(line), flush=True)
     del sim
     if world > 1:
         dist.destroy_process_group()
 
 
-def run_sedov(args):
-    """3D Sedov blast, 512^3 (5 vars, PPM + HLL, SSPRK3): K device-driven steps."""
+def measure_sedov(n, precision, steps, warmup):
+    """3D Sedov blast n^3 (5 vars, PPM + HLL, SSPRK3, CFL 0.8/3): K
+    device-driven steps with inputs resident; returns a dict."""
     import torch
     from mosscap_b200 import problems as P
     from mosscap_b200.hydro import HydroSim
-    n = args.n if args.n != N_CELLS_SIDE else 512
     p = P.sedov_3d(n).with_scheme(max_time=1e30, output_delta=1e30)
-    sim = HydroSim(p, precision=args.precision)
+    sim = HydroSim(p, precision=precision)
+    p.Q = None
     sim.fill_bcs()
-    sim.advance(args.warmup, log_dt=False)
+    sim.advance(warmup, log_dt=False)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     sim.profile_stages(True)
     e0.record()
-    done = len(sim.advance(args.steps, log_dt=False))
+    done = len(sim.advance(steps, log_dt=False))
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     plane_ms, plane_n = sim.stage_time(0)
     z_ms, z_n = sim.stage_time(1)
+    sim.profile_stages(False)
+    flags = sim.status()
+    sim.close()
+    del sim
+    torch.cuda.empty_cache()
     cells = n ** 3
     alg = cells * (3 * 3 - 1) * 5 * 8 / 3.0  # per stage, both passes together
     peak, kind = measured_peak_hbm()
-    line = {"metric": METRIC, "value": cells * done / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": done,
-            "warmup": args.warmup, "ms_per_step": ms / max(done, 1), "higher_is_better": True,
-            "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
-            "config": {"workload": f"sedov_3d_{n}^3_ppm_mc_hll_ssprk3_cfl0.267_{args.precision}"},
+    stage_ms = (plane_ms + z_ms) / max(plane_n, 1)
+    achieved = alg / (stage_ms / 1e3) / 1e9
+    return {"workload": f"sedov_3d_{n}^3_ppm_mc_hll_ssprk3_cfl0.267_{precision}", "value": cells * done / (ms / 1e3),
+            "unit": UNIT, "steps": done, "warmup": warmup, "ms_per_step": ms / max(done, 1),
+            "dtype": "f64" if precision == "fp64" else "f32+f64",
             "kernels": {"plane_pass_ms_avg": plane_ms / max(plane_n, 1), "z_pass_ms_avg": z_ms / max(z_n, 1)},
-            "roofline": {"bound": "hbm", "achieved": alg / ((plane_ms + z_ms) / max(plane_n, 1) / 1e3) / 1e9,
-                         "peak": peak, "unit": "GB/s", "peak_source": kind,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": kind,
+                         "alg_bytes_per_stage": alg,
                          "note": "algorithmic state bytes per stage / (plane pass + z pass) time"},
-            "status_flags": sim.status()}
+            "status_flags": int(flags)}
+
+
+def run_sedov(args):
+    """3D Sedov blast, 512^3 (5 vars, PPM + HLL, SSPRK3): K device-driven steps."""
+    n = args.n if args.n != N_CELLS_SIDE else 512
+    r = measure_sedov(n, args.precision, args.steps, args.warmup)
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": r["steps"],
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+            "dtype": r["dtype"], "data": "synthetic", "config": {"workload": r["workload"]},
+            "kernels": r["kernels"], "roofline": r["roofline"], "status_flags": r["status_flags"]}
     print(json.dumps(line), flush=True)
+
+
+def measure_batch(problems, precision, steps, warmup):
+    """Batched independent problems (one persistent launch per stage kind,
+    graph-replayed steps, autotuned schedule); returns a dict."""
+    import torch
+    from mosscap_b200.hydro import BatchSim
+    cells = sum(p.interior_cells for p in problems)
+    b = BatchSim(problems, precision=precision)
+    b.fill_bcs()
+    t0 = time.perf_counter()
+    sched = b.tune()
+    tune_s = time.perf_counter() - t0
+    b.advance(warmup)
+    _, k0, _ = b.clocks()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    b.advance(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    _, nsteps, status = b.clocks()
+    updates = sum(p.interior_cells * int(k - k_) for p, k, k_ in zip(problems, nsteps, k0))
+    b.close()
+    del b
+    torch.cuda.empty_cache()
+    return {"value": updates / (ms / 1e3), "unit": UNIT, "steps": steps, "warmup": warmup,
+            "ms_per_step": ms / max(steps, 1), "dtype": "f64" if precision == "fp64" else "f32+f64",
+            "problems": len(problems), "interior_cells": cells, "schedule": sched, "tune_s": tune_s,
+            "problems_flagged": int((status != 0).sum())}
 
 
 def run_batch(args):
     """Batched independent Riemann problems: 2048 1D (64..4096 cells) and 2048
     2D quadrant problems (64^2..512^2), MUSCL / minmod, rk2, own dt each."""
-    import torch
     from mosscap_b200 import problems as P
-    from mosscap_b200.hydro import BatchSim
     half = max(args.problems // 2, 1)
     probs = P.riemann_batch(seed=0, n1d=half, n2d=half, riemann_solver=args.solver)
-    cells = sum(p.interior_cells for p in probs)
-    b = BatchSim(probs, precision=args.precision)
-    b.fill_bcs()
-    sched = b.tune()
-    b.advance(args.warmup)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    b.advance(args.steps)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    _, nsteps, status = b.clocks()
-    updates = sum(p.interior_cells * int(k - args.warmup) for p, k in zip(probs, nsteps))
-    line = {"metric": METRIC, "value": updates / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / max(args.steps, 1), "higher_is_better": True,
-            "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+    r = measure_batch(probs, args.precision, args.steps, args.warmup)
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+            "dtype": r["dtype"], "data": "synthetic",
             "config": {"workload": f"riemann_batch_{half}x1d_{half}x2d_muscl_minmod_{args.solver}_rk2_{args.precision}",
-                       "problems": len(probs), "interior_cells": cells, "schedule": sched},
-            "problems_flagged": int((status != 0).sum())}
+                       "problems": r["problems"], "interior_cells": r["interior_cells"], "schedule": r["schedule"]},
+            "problems_flagged": r["problems_flagged"]}
     print(json.dumps(line), flush=True)
 
 
-def run_adjoint(args):
-    """Adjoint of KH 512^2 (WENO5-Z + HLLC, SSPRK3, FP64): forward run of K
-    steps with checkpoints every 20, then the reverse sweep; reports the
-    adjoint : forward cost ratio (CUDA events on the launching stream, mean of
-    3 repetitions after warm-up) and a finite-difference check of the
-    gradient along --fd-directions random directions."""
+def measure_adjoint(n, steps, fd_directions, warmup=3, checkpoint_every=20):
+    """Adjoint of KH n^2 (WENO5-Z + HLLC, SSPRK3, FP64): the gradient of
+    J = 1/2 |rho - rho_target|^2 with respect to the initial vy field and
+    gamma through the autograd wrapper, the adjoint : forward cost ratio of
+    the C ABI calls (CUDA events on the launching stream, mean of 3
+    repetitions after warm-up) and a central finite-difference check along
+    random directions. Returns a dict."""
+    import ctypes
     import torch
     from mosscap_b200 import problems as P
-    import ctypes
     from mosscap_b200 import capi
     from mosscap_b200.adjoint import EulerSteps, _Runner, kh_initial_state, kh_vy, pad_periodic
-    n = args.n if args.n != N_CELLS_SIDE else 512
-    steps = args.steps
     p = P.kelvin_helmholtz_2d(n, seed=0)
     pt = P.kelvin_helmholtz_2d(n, seed=1)
     dev = torch.device("cuda")
@@ -444,13 +508,13 @@ def run_adjoint(args):
     # gradient through the autograd wrapper (the user-facing call)
     vy = torch.tensor(kh_vy(p), device=dev, requires_grad=True)
     g = torch.tensor(p.gamma, dtype=torch.float64, device=dev, requires_grad=True)
-    q = EulerSteps.apply(kh_initial_state(vy, g, p), g, p, steps, 20)
+    q = EulerSteps.apply(kh_initial_state(vy, g, p), g, p, steps, checkpoint_every)
     J = 0.5 * ((q[0] - rho_t) ** 2).sum()
     J.backward()
     # cost: the C ABI calls on one mc_adjoint whose buffers a warm-up pass
-    # allocated; forward = mc_adjoint_forward (K steps, checkpoints every 20),
+    # allocated; forward = mc_adjoint_forward (K steps with checkpoints),
     # adjoint = mc_adjoint_backward (segment recompute + reverse sweep)
-    runner = _Runner(p, p.gamma, 20)
+    runner = _Runner(p, p.gamma, checkpoint_every)
     ng = p.ng
     with torch.no_grad():
         q0 = pad_periodic(kh_initial_state(vy.detach(), g.detach(), p), ng)
@@ -472,7 +536,7 @@ def run_adjoint(args):
         if rec:
             rec[3].record()
 
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(max(warmup, 3)):
         one()
     reps = 3
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(reps)]
@@ -499,7 +563,7 @@ def run_adjoint(args):
         return float((0.5 * (rp - rm) * (rp + rm - 2.0 * rho_t)).sum()) / (2 * eps)
 
     rels, fds, ads = [], [], []
-    for _ in range(args.fd_directions):
+    for _ in range(fd_directions):
         dvy = torch.tensor(rng.standard_normal((n, n)), device=dev)
         dvy = dvy / dvy.norm()
         dg = float(rng.standard_normal()) * 1e-2
@@ -509,21 +573,126 @@ def run_adjoint(args):
         fds.append(fd)
         ads.append(ad)
     fds, ads = np.array(fds), np.array(ads)
-    fd_check = {"directions": len(rels), "eps": {"vy": 1e-7, "gamma": 1e-6}, "direction": "unit vy field, gamma 1e-2 N(0,1)"}
+    fd_check = {"directions": len(rels), "eps": {"vy": 1e-7, "gamma": 1e-6},
+                "direction": "unit vy field, gamma 1e-2 N(0,1)"}
     if rels:
         fd_check.update({"max_rel_err": max(rels), "median_rel_err": float(np.median(rels)),
                          "n_within_1e-5": int(sum(r <= 1e-5 for r in rels)),
                          "aggregate_rel_err": float(np.linalg.norm(fds - ads) / np.linalg.norm(ads)),
                          "max_abs_err": float(np.abs(fds - ads).max())})
-    line = {"metric": "adjoint:forward cost", "value": bwd / fwd, "unit": "ratio", "n_gpus": 1, "steps": steps,
-            "higher_is_better": False, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"kh_2d_{n}x{n}_weno5z_hllc_ssprk3_adjoint_ckpt20", "loss": "1/2 |rho - rho_target|^2",
-                       "gradient": "initial vy field and gamma"},
-            "forward_ms": fwd, "backward_ms": bwd,
-            "forward_zone_updates_per_s": n * n * steps / (fwd / 1e3),
-            "loss": J.item(), "dgamma": g.grad.item(), "grad_vy_norm": vy.grad.norm().item(),
-            "fd_check": fd_check}
+    out = {"workload": f"kh_2d_{n}x{n}_weno5z_hllc_ssprk3_adjoint_ckpt{checkpoint_every}", "steps": steps,
+           "adjoint_forward_ratio": bwd / fwd, "forward_ms": fwd, "backward_ms": bwd,
+           "forward_zone_updates_per_s": n * n * steps / (fwd / 1e3),
+           "loss": J.item(), "dgamma": g.grad.item(), "grad_vy_norm": vy.grad.norm().item(),
+           "fd_check": fd_check}
+    del runner
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_adjoint(args):
+    """Adjoint of KH 512^2 (WENO5-Z + HLLC, SSPRK3, FP64): forward run of K
+    steps with checkpoints every 20, then the reverse sweep; reports the
+    adjoint : forward cost ratio and a finite-difference check of the
+    gradient along --fd-directions random directions."""
+    n = args.n if args.n != N_CELLS_SIDE else 512
+    r = measure_adjoint(n, args.steps, args.fd_directions, args.warmup)
+    line = {"metric": "adjoint:forward cost", "value": r["adjoint_forward_ratio"], "unit": "ratio", "n_gpus": 1,
+            "steps": args.steps, "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": r["workload"], "loss": "1/2 |rho - rho_target|^2",
+                       "gradient": "initial vy field and gamma"}}
+    line.update({k: v for k, v in r.items() if k not in ("workload", "steps", "adjoint_forward_ratio")})
     print(json.dumps(line), flush=True)
+
+
+def measure_kh_form(n, precision, steps, warmup, rho_ref=None):
+    """KH n^2 in the given precision form, device-driven loop with inputs
+    resident; the density after warmup + steps steps is compared with
+    rho_ref (the FP64 run's after the same number of steps), if given."""
+    import torch
+    from mosscap_b200 import problems as P
+    from mosscap_b200.hydro import HydroSim
+    p = P.kelvin_helmholtz_2d(n, seed=0)
+    sim = HydroSim(p, precision=precision)
+    sim.fill_bcs()
+    sim.advance(warmup, log_dt=False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    sim.profile_stages(True)
+    e0.record()
+    done = len(sim.advance(steps, log_dt=False))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    stage_ms, stage_n = sim.stage_time(0)
+    sim.profile_stages(False)
+    out = {"value": n * n * done / (ms / 1e3), "unit": UNIT, "steps": done, "warmup": warmup,
+           "ms_per_step": ms / max(done, 1), "stage_ms_avg": stage_ms / max(stage_n, 1),
+           "status_flags": int(sim.status())}
+    if rho_ref is not None:
+        ng = p.ng
+        rho = sim.Q[0, 0, ng:-ng, ng:-ng]
+        d = (rho - rho_ref).abs()
+        out["density_rel_l1_vs_fp64"] = float(d.sum() / rho_ref.abs().sum())
+        out["density_rel_linf_vs_fp64"] = float(d.max() / rho_ref.abs().max())
+        out["error_after_steps"] = warmup + done
+    sim.close()
+    return out
+
+
+def run_extras(args, rho64, value64):
+    """The forms beside the headline, measured in the same run (1 GPU):
+    the FP32 compute form on the headline problem, Sedov 512^3 in FP64 and
+    FP32, the 4096-problem batch in FP64 and FP32, and the adjoint at 512^2
+    for a reduced step count. Each failure is recorded, not raised."""
+    import torch
+    from mosscap_b200 import problems as P
+    ex = {}
+
+    def guarded(name, fn):
+        t0 = time.perf_counter()
+        try:
+            ex[name] = fn()
+        except Exception as e:  # recorded in the line; the headline stands
+            ex[name] = {"error": f"{type(e).__name__}: {e}"}
+        ex[name]["wall_s"] = round(time.perf_counter() - t0, 2)
+        torch.cuda.empty_cache()
+
+    def fp32():
+        r = measure_kh_form(args.n, "fp32", args.steps, args.warmup, rho_ref=rho64)
+        r["speedup_vs_fp64"] = r["value"] / value64
+        r["workload"] = f"kelvin_helmholtz_2d_{args.n}x{args.n}_weno5z_hllc_ssprk3_fp32_form"
+        return r
+
+    guarded("fp32_form", fp32)
+
+    def sedov():
+        steps = max(2, min(args.steps, 5))
+        r64 = measure_sedov(512, "fp64", steps, 1)
+        r32 = measure_sedov(512, "fp32", steps, 1)
+        r64["fp32_form"] = {"value": r32["value"], "ms_per_step": r32["ms_per_step"],
+                            "kernels": r32["kernels"], "status_flags": r32["status_flags"],
+                            "speedup_vs_fp64": r32["value"] / r64["value"]}
+        return r64
+
+    guarded("sedov3d", sedov)
+
+    def batch():
+        probs = P.riemann_batch(seed=0, n1d=2048, n2d=2048, riemann_solver="hllc")
+        steps = max(3, min(args.steps, 10))
+        r = {"workload": "riemann_batch_2048x1d_2048x2d_muscl_minmod_hllc_rk2",
+             "fp64": measure_batch(probs, "fp64", steps, 2),
+             "fp32": measure_batch(probs, "fp32", steps, 2)}
+        r["fp32_speedup"] = r["fp32"]["value"] / r["fp64"]["value"]
+        return r
+
+    guarded("batch", batch)
+
+    def adjoint():
+        return measure_adjoint(512, 40, 8)
+
+    guarded("adjoint", adjoint)
+    return ex
 
 
 def main():

@@ -348,7 +348,7 @@ mc_status mc_adjoint_backward(mc_adjoint* adj, double* lambda, double* dgamma, v
  * come from one static device array of 16 MiB that every GPU loading the
  * library holds until the process exits; a problem needs
  * 2 x (2+num_dim+num_tracers) x xc x yc x zc doubles (plus
- * (2+num_dim) x nx x ny x nz in 3D) and is rejected with
+ * (2+num_dim+num_tracers) x nx x ny x nz in 3D) and is rejected with
  * MC_ERR_OUT_OF_MEMORY when that exceeds 16 MiB (a 4-variable 2D grid with
  * 3 ghosts fits up to 506 x 506 interior cells). All faces must be built-in kinds
  * (no user hook without a context). The first call on a device looks up the

@@ -86,25 +86,6 @@ int halo_needed(int rec) {
     return rec == MC_RECON_FOG ? 1 : rec == MC_RECON_MUSCL ? 2 : 3;
 }
 
-// The stage plan of each SSPRK driver (source/TimeStepping.cpp): input and
-// output buffer of each stage (0 = caller's Q, 1 = buffer A, 2 = buffer B)
-// and the combination applied.
-struct StagePlan {
-    int n;
-    int in[4], out[4], combo[4];
-};
-
-StagePlan plan_for(int stepper) {
-    switch (stepper) {
-        case MC_STEPPER_RK2:
-            return {2, {0, 1}, {1, 0}, {mc::kAdd, mc::kRk2Final}};
-        case MC_STEPPER_SSPRK3:
-            return {3, {0, 1, 2}, {1, 2, 0}, {mc::kAdd, mc::kSsp3Second, mc::kSsp3Final}};
-        default:
-            return {4, {0, 1, 2, 1}, {1, 2, 1, 0}, {mc::kHalfAdd, mc::kHalfAdd, mc::kSsp4Third, mc::kHalfAdd}};
-    }
-}
-
 StageParams base_params(const mc_ctx* c) {
     StageParams p;
     std::memset(&p, 0, sizeof(p));
@@ -212,9 +193,20 @@ mc::EosLaunch eos_launch(const mc_ctx* c, const double* q_in, double* q_out, boo
     return L;
 }
 
+// Faces of kind MC_BC_USERFN among the active ones (bit f = face f).
+int user_face_mask(const mc_ctx* c) {
+    int m = 0;
+    for (int f = 0; f < 2 * c->grid.num_dim; ++f) {
+        if (c->grid.bc[f] == MC_BC_USERFN) {
+            m |= 1 << f;
+        }
+    }
+    return m;
+}
+
 // Enqueue one SSPRK step on Q. dt_dev (device-driven loop) or dt (host).
 mc_status enqueue_step(mc_ctx* c, double* Q, double dt, const double* dt_dev, bool reset_min, cudaStream_t s) {
-    const StagePlan plan = plan_for(c->scheme.time_stepper);
+    const mc::StagePlan plan = mc::plan_for(c->scheme.time_stepper);
     double* bufs[3] = {Q, c->buf_a, c->buf_b};
     c->last_stage_in = bufs[plan.in[plan.n - 1]];
     for (int st = 0; st < plan.n; ++st) {
@@ -249,6 +241,15 @@ mc_status enqueue_step(mc_ctx* c, double* Q, double dt, const double* dt_dev, bo
         }
         if (c->user_bc) {
             c->user_bc(c->user_bc_data, p.q_out, (void*)s);
+            // the hook fills the MC_BC_USERFN ghosts after the fused CFL
+            // reduction of the last stage; add their layers to it
+            const int mask = user_face_mask(c);
+            if (p.last && mask) {
+                StageParams g = p;
+                g.q_in = p.q_out;
+                c->launches += 1;
+                MC_CUDA(mc::launch_cfl_min_ghosts(g, c->grid.num_dim, mask, s), "cfl_min (user ghosts)");
+            }
         }
     }
     return MC_OK;

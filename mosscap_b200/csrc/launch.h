@@ -7,6 +7,26 @@
 
 namespace mc {
 
+// The stage plan of each SSPRK driver (source/TimeStepping.cpp: rk2 :39-93,
+// ssprk3 :116-190, ssprk4 :213-308): input and output buffer of each stage
+// (0 = the caller's Q, 1 = stage buffer A, 2 = stage buffer B) and the stage
+// combination applied. Every stage also reads the step-start state Q.
+struct StagePlan {
+    int n;
+    int in[4], out[4], combo[4];
+};
+
+inline StagePlan plan_for(int stepper) {
+    switch (stepper) {
+        case 0:  // rk2
+            return {2, {0, 1}, {1, 0}, {kAdd, kRk2Final}};
+        case 1:  // ssprk3
+            return {3, {0, 1, 2}, {1, 2, 0}, {kAdd, kSsp3Second, kSsp3Final}};
+        default:  // ssprk4
+            return {4, {0, 1, 2, 1}, {1, 2, 1, 0}, {kHalfAdd, kHalfAdd, kSsp4Third, kHalfAdd}};
+    }
+}
+
 // One stage of an SSPRK step. pass selects, in 3D, the x-y plane pass (0)
 // or the z pass that finishes the stage (1); it is ignored in 1D and 2D.
 cudaError_t launch_stage_d1_fp64(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
@@ -31,6 +51,9 @@ cudaError_t launch_cons_to_prim(const StageParams& p, double* w, int ndim, cudaS
 // CFL minimum over every cell of Q (ghosts included) into blk->cfl_min_bits,
 // which the launch first resets.
 cudaError_t launch_cfl_min(const StageParams& p, int ndim, cudaStream_t s);
+// CFL minimum over the ghost layers of the faces in face_mask (bit f = face
+// f), folded into blk->cfl_min_bits without a reset.
+cudaError_t launch_cfl_min_ghosts(const StageParams& p, int ndim, int face_mask, cudaStream_t s);
 // Device-driven loop bookkeeping (see util_kernels.cu).
 cudaError_t launch_clock_init(DeviceBlock* blk, double time, double max_time, double prev_output_time,
                               double output_delta, double max_cfl, cudaStream_t s);

@@ -110,9 +110,8 @@ mc_status validate(const mc_grid& g, const mc_scheme& s) {
             return fail(MC_ERR_INVALID_ARGUMENT, "bad extents: each active axis needs ng interior cells");
         }
     }
-    if (g.num_tracers < 0 || 2 + g.num_dim + g.num_tracers > mc::kMaxVars ||
-        (g.num_dim == 3 && g.num_tracers > 0)) {
-        return fail(MC_ERR_INVALID_ARGUMENT, "unsupported number of variables");
+    if (g.num_tracers < 0 || 2 + g.num_dim + g.num_tracers > mc::kMaxVars) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "too many variables (at most 8)");
     }
     if (!(g.dx > 0.0) || !std::isfinite(g.dx) || !std::isfinite(s.gamma)) {
         return fail(MC_ERR_INVALID_ARGUMENT, "dx and gamma must be finite (dx > 0)");
@@ -123,7 +122,7 @@ mc_status validate(const mc_grid& g, const mc_scheme& s) {
             return fail(MC_ERR_INVALID_ARGUMENT, "boundary kind must be a built-in one");
         }
         if (g.bc[f] == MC_BC_CONSTANT && 2 + g.num_dim + g.num_tracers > 5) {
-            return fail(MC_ERR_INVALID_ARGUMENT, "constant boundaries hold at most 5 variables");
+            return fail(MC_ERR_UNSUPPORTED, "constant boundaries hold at most 5 variables");
         }
     }
     for (int a = 0; a < g.num_dim; ++a) {
@@ -178,22 +177,15 @@ mc_status mc_time_step_noalloc(const mc_grid* grid, const mc_scheme* scheme, dou
         return st;
     }
     double* bufs[3] = {Q, sym->scratch, sym->scratch + state};
-    // stage plans of the SSPRK drivers (source/TimeStepping.cpp): input and
-    // output buffer per stage (0 = Q, 1 = A, 2 = B) and the combination
-    static const int n_st[3] = {2, 3, 4};
-    static const int in_b[3][4] = {{0, 1}, {0, 1, 2}, {0, 1, 2, 1}};
-    static const int out_b[3][4] = {{1, 0}, {1, 2, 0}, {1, 2, 1, 0}};
-    static const int combo[3][4] = {{mc::kAdd, mc::kRk2Final},
-                                    {mc::kAdd, mc::kSsp3Second, mc::kSsp3Final},
-                                    {mc::kHalfAdd, mc::kHalfAdd, mc::kSsp4Third, mc::kHalfAdd}};
-    const int ts = s.time_stepper;
+    // the same stage plan as the context path (launch.h)
+    const mc::StagePlan plan = mc::plan_for(s.time_stepper);
     const cudaStream_t cs = static_cast<cudaStream_t>(stream);
-    for (int k = 0; k < n_st[ts]; ++k) {
+    for (int k = 0; k < plan.n; ++k) {
         mc::StageParams p;
         std::memset(&p, 0, sizeof(p));
-        p.q_in = bufs[in_b[ts][k]];
+        p.q_in = bufs[plan.in[k]];
         p.q_old = Q;
-        p.q_out = bufs[out_b[ts][k]];
+        p.q_out = bufs[plan.out[k]];
         p.dqxy = g.num_dim == 3 ? sym->scratch + 2 * state : nullptr;
         p.xc = g.xc;
         p.yc = g.yc;
@@ -209,8 +201,8 @@ mc_status mc_time_step_noalloc(const mc_grid* grid, const mc_scheme* scheme, dou
         p.gamma = s.gamma;
         p.dt = dt;
         p.dt_dev = nullptr;
-        p.combo = combo[ts][k];
-        p.last = k == n_st[ts] - 1;
+        p.combo = plan.combo[k];
+        p.last = k == plan.n - 1;
         // the block keeps the last call's contents: the first stage clears the
         // CFL-minimum cell that the last stage reduces into
         p.reset_min = k == 0;

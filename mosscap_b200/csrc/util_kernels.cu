@@ -68,6 +68,50 @@ __global__ void __launch_bounds__(256) cfl_min_kernel(StageParams p) {
     block_publish(m, flags, true, p.blk, red_d, red_u);
 }
 
+// The CFL minimum over the ghost layers of the faces in face_mask (bit f =
+// face f: xs, xe, ys, ye, zs, ze), whole extent along the other axes,
+// folded into blk->cfl_min_bits without a reset. The fused stage kernels
+// reduce over every value they write; the ghosts of MC_BC_USERFN faces are
+// written afterwards by the caller's hook, and compute_dt reads every cell
+// (source/Hydro.cpp:209-229), so those layers are added here.
+template <int NDIM>
+__global__ void __launch_bounds__(256) cfl_min_ghosts_kernel(StageParams p, int face_mask) {
+    constexpr int nh = 2 + NDIM;
+    __shared__ double red_d[8];
+    __shared__ unsigned red_u[8];
+    double m = __longlong_as_double((long long)kInfBits);
+    unsigned flags = 0;
+    const int ext[3] = {p.xc, p.yc, p.zc};
+    for (int f = 0; f < 2 * NDIM; ++f) {
+        if (!(face_mask & (1 << f))) {
+            continue;
+        }
+        const int a = f >> 1;
+        int lo[3] = {0, 0, 0}, n[3] = {ext[0], ext[1], ext[2]};
+        lo[a] = (f & 1) ? ext[a] - p.ng : 0;
+        n[a] = p.ng;
+        const long long cells = (long long)n[0] * n[1] * n[2];
+        for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < cells;
+             c += (long long)gridDim.x * blockDim.x) {
+            const int i = lo[0] + (int)(c % n[0]);
+            const long long r = c / n[0];
+            const int j = lo[1] + (int)(r % n[1]);
+            const int k = lo[2] + (int)(r / n[1]);
+            double q[nh], w[nh];
+            bool fin = true;
+#pragma unroll
+            for (int v = 0; v < nh; ++v) {
+                q[v] = p.q_in[qidx(p, v, k, j, i)];
+                fin = fin && isfinite(q[v]);
+            }
+            prim_from_cons<NDIM>(p.gamma, q, w);
+            flags |= state_flags(w[0], w[nh - 1], fin);
+            m = smin(cfl_dt<NDIM>(p.gamma, p.dx, w), m);
+        }
+    }
+    block_publish(m, flags, true, p.blk, red_d, red_u);
+}
+
 __global__ void reset_min_kernel(DeviceBlock* blk) {
     blk->cfl_min_bits = kInfBits;
 }
@@ -162,6 +206,22 @@ cudaError_t launch_cfl_min(const StageParams& p, int ndim, cudaStream_t s) {
             break;
         default:
             cfl_min_kernel<3><<<blocks, 256, 0, s>>>(p);
+            break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cfl_min_ghosts(const StageParams& p, int ndim, int face_mask, cudaStream_t s) {
+    const int blocks = 148;
+    switch (ndim) {
+        case 1:
+            cfl_min_ghosts_kernel<1><<<blocks, 256, 0, s>>>(p, face_mask);
+            break;
+        case 2:
+            cfl_min_ghosts_kernel<2><<<blocks, 256, 0, s>>>(p, face_mask);
+            break;
+        default:
+            cfl_min_ghosts_kernel<3><<<blocks, 256, 0, s>>>(p, face_mask);
             break;
     }
     return cudaGetLastError();

@@ -24,10 +24,15 @@ from typing import Optional, Sequence
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# The reference's source tree (its ``source/`` directory), read only when the
+# reference build is made; MOSSCAP_REFERENCE_SOURCE overrides the default.
+REF_SOURCE = os.environ.get("MOSSCAP_REFERENCE_SOURCE", "/root/reference/source")
 LIB_PATHS = {
     "reference": os.path.join(HERE, "_ref", "libmosscap_ref.so"),
     "port": os.path.join(HERE, "liboracle_port.so"),
 }
+# The adapter check program (oracle/adapter_check.cpp), built with the reference.
+ADAPTER_CHECK = os.path.join(HERE, "_ref", "adapter_check")
 
 # Reference enum ordinals (source/Reconstruct.hpp:10-27, source/Riemann.hpp:10-14,
 # source/TimeStepping.hpp:10-14, source/State.hpp:62-70).
@@ -74,9 +79,16 @@ EOS_TYPE = {"ideal": 0, "analyticlteh": 1, "tabulatedlteh": 2}
 
 
 def build(kind: str = "all") -> None:
-    """Build the oracle libraries with ``oracle/Makefile`` (``make port|ref``)."""
-    targets = ["port", "ref"] if kind == "all" else [kind]
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    """Build the oracle libraries with ``oracle/Makefile`` (``make port|ref|adapter``;
+    ``adapter`` links the product library, which must be built first)."""
+    targets = ["port", "ref", "adapter"] if kind == "all" else [kind]
+    subprocess.run(["make", "-s", "-C", HERE, f"REF_SRC={REF_SOURCE}"] + targets, check=True)
+
+
+def have_reference_sources() -> bool:
+    """Whether the reference's source tree is present (it is not on every
+    machine that runs the tests; the built libraries travel instead)."""
+    return os.path.isdir(REF_SOURCE)
 
 
 _LIBS: dict = {}

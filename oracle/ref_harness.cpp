@@ -40,6 +40,12 @@ Mosscap::Simulation& S(void* p) {
 
 } // namespace
 
+// The Simulation a handle holds (C++ linkage; oracle/adapter_check.cpp
+// installs the C++ hook adapter on it).
+Mosscap::Simulation* moracle_simulation(void* p) {
+    return &S(p);
+}
+
 extern "C" {
 
 void* moracle_create(const moracle_config* c) {

@@ -17,7 +17,20 @@
 //  - Kokkos::parallel_for / parallel_reduce over a flat index range, run with
 //    OpenMP; Kokkos::Min joins with `src < dest ? src : dest` starting from the
 //    reduction identity (the largest finite value).
+//  - yakl::Array(label, pointer, dims...) wraps memory it does not own.
+//
+// With MOSSCAP_SHIM_MANAGED defined, memDevice arrays are allocated as CUDA
+// managed memory, which a GPU kernel and the host loops can both address:
+// the arrays of a Simulation are then device memory, as in Mosscap's CUDA
+// build, so the C++ hook adapter can be run against the reference's own
+// Simulation type (the adapter check in oracle/adapter_check.cpp).
 #pragma once
+
+#ifdef MOSSCAP_SHIM_MANAGED
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstdlib>
+#endif
 
 #include <atomic>
 
@@ -203,8 +216,31 @@ public:
             dims_[i] = d[i];
             total *= d[i];
         }
+#ifdef MOSSCAP_SHIM_MANAGED
+        if (myMem == memDevice) {
+            NC* p = nullptr;
+            if (cudaMallocManaged(reinterpret_cast<void**>(&p), sizeof(NC) * (total > 0 ? total : 1)) !=
+                cudaSuccess) {
+                std::fprintf(stderr, "yakl shim: cudaMallocManaged failed for %s\n", label);
+                std::abort();
+            }
+            std::memset(static_cast<void*>(p), 0, sizeof(NC) * total);
+            owner_ = std::shared_ptr<NC[]>(p, [](NC* x) { cudaFree(x); });
+            ptr_ = owner_.get();
+            return;
+        }
+#endif
         owner_ = std::shared_ptr<NC[]>(new NC[total]());
         ptr_ = owner_.get();
+    }
+
+    // A view of memory the array does not own (YAKL's unmanaged form).
+    template <class... Ints, std::enable_if_t<sizeof...(Ints) == rank, int> = 0>
+    Array(const char* label, T* data, Ints... n) : ptr_(data), label_(label) {
+        const int64_t d[rank] = {int64_t(n)...};
+        for (int i = 0; i < rank; ++i) {
+            dims_[i] = d[i];
+        }
     }
 
     template <class... Ints>

@@ -18,7 +18,8 @@ def pytest_configure(config):
 
 
 def _have_ref_sources() -> bool:
-    return os.path.isdir("/root/reference/source")
+    from oracle import oracle as O
+    return O.have_reference_sources()
 
 
 @pytest.fixture(scope="session")
