@@ -315,8 +315,13 @@ __device__ __forceinline__ void riemann(T gamma, T gfac, int axis, const T* wL, 
         const T rho_avg = T(0.5) * (wL[0] + wR[0]);
         const T cs_avg = T(0.5) * (csL + csR);
         const T p_mid = T(0.5) * (pL + pR + (vL - vR) * rho_avg * cs_avg);
-        const T cLstar = (p_mid <= pL) ? T(1) : sqrt(T(1) + gfac * (p_mid / pL - T(1)));
-        const T cRstar = (p_mid <= pR) ? T(1) : sqrt(T(1) + gfac * (p_mid / pR - T(1)));
+        // both shock factors are evaluated and then selected: the lanes of a
+        // warp disagree on the branch in most faces, and a straight-line
+        // sequence lets the two square roots overlap (values unchanged)
+        const T sqL = sqrt(T(1) + gfac * (p_mid / pL - T(1)));
+        const T sqR = sqrt(T(1) + gfac * (p_mid / pR - T(1)));
+        const T cLstar = (p_mid <= pL) ? T(1) : sqL;
+        const T cRstar = (p_mid <= pR) ? T(1) : sqR;
         const T aL = vL - csL * cLstar;
         const T aR = vR + csR * cRstar;
         const T bM = smin(-tiny, aL);
@@ -344,16 +349,15 @@ __device__ __forceinline__ void riemann(T gamma, T gfac, int axis, const T* wL, 
         add_along<NDIM>(fR, axis, pR);
         fL[ie] = qL[ie] * vxL + pL * vL;
         fR[ie] = qR[ie] * vxR + pR * vR;
-        T sL, sR, sM;
-        if (aM >= T(0)) {
-            sL = aM / (aM - bM);
-            sR = T(0);
-            sM = -bM / (aM - bM);
-        } else {
-            sL = T(0);
-            sR = -aM / (bP - aM);
-            sM = bP / (bP - aM);
-        }
+        // aM >= 0: sL = aM / (aM - bM), sR = 0, sM = -bM / (aM - bM);
+        // otherwise sL = 0, sR = -aM / (bP - aM), sM = bP / (bP - aM):
+        // the same two quotients, with their operands selected first
+        const bool left = aM >= T(0);
+        const T den = left ? (aM - bM) : (bP - aM);
+        const T s_out = (left ? aM : -aM) / den;
+        const T sM = (left ? -bM : bP) / den;
+        const T sL = left ? s_out : T(0);
+        const T sR = left ? T(0) : s_out;
 #pragma unroll
         for (int i = 0; i < nh; ++i) {
             flux[i] = sL * fL[i] + sR * fR[i];

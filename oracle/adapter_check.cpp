@@ -23,6 +23,7 @@
 #include "TimeStepping.hpp"
 #include "Boundaries.hpp"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -68,7 +69,10 @@ void write_file(const std::string& path, const void* data, size_t bytes) {
 
 // A user boundary of the kind a Mosscap problem generator installs: the
 // ghost cells of the x-start face (all of them, edges and corners included)
-// take a fixed inflow state whose density follows sim.dt_sub.
+// take a fixed inflow state whose density follows sim.dt_sub. In Mosscap's
+// CUDA build a user_bc fills device memory with a device loop; the shim's
+// loops run on the host, so the ghost runs are written with cudaMemcpy, which
+// reaches the library's device stage buffers as well as managed memory.
 void inflow_user_bc(const Mosscap::Simulation& sim) {
     const auto& Q = sim.state.Q;
     const auto& sz = sim.state.sz;
@@ -92,11 +96,15 @@ void inflow_user_bc(const Mosscap::Simulation& sim) {
         ie = 4;
     }
     q[ie] = p / (gamma - 1.0) + 0.5 * rho * v2;
-    for (int k = 0; k < sz.zc; ++k) {
-        for (int j = 0; j < sz.yc; ++j) {
-            for (int i = 0; i < sz.ng; ++i) {
-                for (int v = 0; v <= ie; ++v) {
-                    Q(v, k, j, i) = q[v];
+    std::vector<double> run(static_cast<size_t>(sz.ng));
+    for (int v = 0; v <= ie; ++v) {
+        std::fill(run.begin(), run.end(), q[v]);
+        for (int k = 0; k < sz.zc; ++k) {
+            for (int j = 0; j < sz.yc; ++j) {
+                if (cudaMemcpy(&Q(v, k, j, 0), run.data(), sizeof(double) * run.size(), cudaMemcpyDefault) !=
+                    cudaSuccess) {
+                    std::fprintf(stderr, "adapter_check: user_bc copy failed\n");
+                    std::exit(3);
                 }
             }
         }
