@@ -486,13 +486,15 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
-def measure_adjoint(n, steps, fd_directions, warmup=3, checkpoint_every=20):
+def measure_adjoint(n, steps, fd_directions, warmup=3, checkpoint_every=20, tlm_directions=0, eps_ladder=False):
     """Adjoint of KH n^2 (WENO5-Z + HLLC, SSPRK3, FP64): the gradient of
     J = 1/2 |rho - rho_target|^2 with respect to the initial vy field and
     gamma through the autograd wrapper, the adjoint : forward cost ratio of
     the C ABI calls (CUDA events on the launching stream, mean of 3
-    repetitions after warm-up) and a central finite-difference check along
-    random directions. Returns a dict."""
+    repetitions after warm-up), the gradient against the tangent-linear model
+    on tlm_directions random directions and against central finite
+    differences on the first fd_directions of them (with eps_ladder, the
+    finite-difference misses re-run over a ladder of steps). Returns a dict."""
     import ctypes
     import torch
     from mosscap_b200 import problems as P
@@ -546,11 +548,41 @@ def measure_adjoint(n, steps, fd_directions, warmup=3, checkpoint_every=20):
     torch.cuda.synchronize()
     fwd = sum(x[0].elapsed_time(x[1]) for x in ev) / reps
     bwd = sum(x[2].elapsed_time(x[3]) for x in ev) / reps
-    # central finite differences along random unit directions of (vy, gamma):
-    # the vy part with a step below the gap between near-tied CFL arg-min
-    # candidates, the gamma part with a step clear of roundoff
+    # random unit directions of (vy, gamma): the adjoint gradient against the
+    # tangent-linear model (mc_tangent_linear, forward-mode dual numbers
+    # through the forward arithmetic) on every direction, and against
+    # central finite differences on the first fd_directions of them
+    from mosscap_b200.adjoint import kh_directional_derivatives
     gvy, gg = vy.grad.detach(), g.grad.item()
     rng = np.random.default_rng(2)
+    ndir = max(fd_directions, tlm_directions)
+    dirs, dgs = [], []
+    for _ in range(ndir):
+        dvy = torch.tensor(rng.standard_normal((n, n)), device=dev)
+        dirs.append(dvy / dvy.norm())
+        dgs.append(float(rng.standard_normal()) * 1e-2)
+    ads = np.array([float((gvy * d).sum()) + gg * dg for d, dg in zip(dirs, dgs)])
+
+    def rel(a, b):
+        return np.abs(a - b) / np.maximum(np.maximum(np.abs(a), np.abs(b)), 1e-300)
+
+    tlm_check = None
+    tls = None
+    if tlm_directions:
+        t0 = time.perf_counter()
+        tls = []
+        for c0 in range(0, tlm_directions, 16):
+            c1 = min(c0 + 16, tlm_directions)
+            Jt, dJ = kh_directional_derivatives(p, vy.detach(), p.gamma, torch.stack(dirs[c0:c1]), dgs[c0:c1],
+                                                rho_t, steps)
+            tls.extend(dJ)
+        tls = np.array(tls)
+        r = rel(ads[:tlm_directions], tls)
+        tlm_check = {"directions": tlm_directions, "max_rel_err": float(r.max()), "median_rel_err": float(np.median(r)),
+                     "n_within_1e-5": int((r <= 1e-5).sum()), "n_within_1e-8": int((r <= 1e-8).sum()),
+                     "loss_rel_diff": abs(Jt - J.item()) / J.item(), "seconds": time.perf_counter() - t0,
+                     "how": "mc_tangent_linear: dual numbers (4 directions per pass) through the forward arithmetic, "
+                            "branches as the forward run takes them"}
 
     def final_rho(vy_, g_):
         with torch.no_grad():
@@ -562,29 +594,38 @@ def measure_adjoint(n, steps, fd_directions, warmup=3, checkpoint_every=20):
         rm = final_rho(vy.detach() - eps * dvy, p.gamma - eps * dg)
         return float((0.5 * (rp - rm) * (rp + rm - 2.0 * rho_t)).sum()) / (2 * eps)
 
-    rels, fds, ads = [], [], []
-    for _ in range(fd_directions):
-        dvy = torch.tensor(rng.standard_normal((n, n)), device=dev)
-        dvy = dvy / dvy.norm()
-        dg = float(rng.standard_normal()) * 1e-2
-        fd = cdiff(dvy, 0.0, 1e-7) + cdiff(0.0 * dvy, dg, 1e-6)
-        ad = float((gvy * dvy).sum()) + gg * dg
-        rels.append(abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
-        fds.append(fd)
-        ads.append(ad)
-    fds, ads = np.array(fds), np.array(ads)
-    fd_check = {"directions": len(rels), "eps": {"vy": 1e-7, "gamma": 1e-6},
+    fds = np.array([cdiff(dirs[k], 0.0, 1e-7) + cdiff(0.0 * dirs[k], dgs[k], 1e-6) for k in range(fd_directions)])
+    fd_check = {"directions": fd_directions, "eps": {"vy": 1e-7, "gamma": 1e-6},
                 "direction": "unit vy field, gamma 1e-2 N(0,1)"}
-    if rels:
-        fd_check.update({"max_rel_err": max(rels), "median_rel_err": float(np.median(rels)),
-                         "n_within_1e-5": int(sum(r <= 1e-5 for r in rels)),
-                         "aggregate_rel_err": float(np.linalg.norm(fds - ads) / np.linalg.norm(ads)),
-                         "max_abs_err": float(np.abs(fds - ads).max())})
+    if fd_directions:
+        r = rel(fds, ads[:fd_directions])
+        fd_check.update({"max_rel_err": float(r.max()), "median_rel_err": float(np.median(r)),
+                         "n_within_1e-5": int((r <= 1e-5).sum()),
+                         "aggregate_rel_err": float(np.linalg.norm(fds - ads[:fd_directions]) /
+                                                    np.linalg.norm(ads[:fd_directions])),
+                         "max_abs_err": float(np.abs(fds - ads[:fd_directions]).max())})
+        if tls is not None and tlm_directions >= fd_directions:
+            fd_check["max_abs_err_vs_tlm"] = float(np.abs(fds - tls[:fd_directions]).max())
+        if eps_ladder:
+            # the directions FD misses by more than 1e-5: the vy part's
+            # absolute error against the tangent-linear value over a ladder of
+            # steps, which shows the FD noise floor (roundoff below ~1e-7,
+            # kinks of the CFL arg-min and of the branches above)
+            ladder = []
+            ref = tls if tls is not None else ads
+            for k in np.nonzero(r > 1e-5)[0]:
+                dg_part = cdiff(0.0 * dirs[k], dgs[k], 1e-6)
+                errs = {f"{e:g}": abs(cdiff(dirs[k], 0.0, e) + dg_part - float(ref[k]))
+                        for e in (1e-8, 1e-7, 1e-6, 1e-5, 1e-4)}
+                ladder.append({"direction": int(k), "derivative": float(ref[k]), "abs_err_by_eps": errs,
+                               "min_abs_err": min(errs.values()),
+                               "min_rel_err": min(errs.values()) / max(abs(float(ref[k])), 1e-300)})
+            fd_check["eps_ladder"] = ladder
     out = {"workload": f"kh_2d_{n}x{n}_weno5z_hllc_ssprk3_adjoint_ckpt{checkpoint_every}", "steps": steps,
            "adjoint_forward_ratio": bwd / fwd, "forward_ms": fwd, "backward_ms": bwd,
            "forward_zone_updates_per_s": n * n * steps / (fwd / 1e3),
            "loss": J.item(), "dgamma": g.grad.item(), "grad_vy_norm": vy.grad.norm().item(),
-           "fd_check": fd_check}
+           "fd_check": fd_check, "tlm_check": tlm_check}
     del runner
     torch.cuda.empty_cache()
     return out
@@ -596,7 +637,8 @@ def run_adjoint(args):
     adjoint : forward cost ratio and a finite-difference check of the
     gradient along --fd-directions random directions."""
     n = args.n if args.n != N_CELLS_SIDE else 512
-    r = measure_adjoint(n, args.steps, args.fd_directions, args.warmup)
+    r = measure_adjoint(n, args.steps, args.fd_directions, args.warmup, tlm_directions=args.fd_directions,
+                        eps_ladder=True)
     line = {"metric": "adjoint:forward cost", "value": r["adjoint_forward_ratio"], "unit": "ratio", "n_gpus": 1,
             "steps": args.steps, "higher_is_better": False, "dtype": "f64", "data": "synthetic",
             "config": {"workload": r["workload"], "loss": "1/2 |rho - rho_target|^2",
@@ -689,7 +731,10 @@ def run_extras(args, rho64, value64):
     guarded("batch", batch)
 
     def adjoint():
-        return measure_adjoint(512, 40, 8)
+        # the full configuration: 512^2, 400 steps, checkpoints every 20;
+        # the gradient against the tangent-linear model on 64 directions
+        # and against finite differences on 8 of them
+        return measure_adjoint(512, 400, 8, tlm_directions=64)
 
     guarded("adjoint", adjoint)
     return ex

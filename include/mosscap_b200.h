@@ -338,6 +338,24 @@ mc_status mc_adjoint_forward(mc_adjoint* adj, double* Q, const mc_clock* clock, 
  * stream when dgamma is not NULL. */
 mc_status mc_adjoint_backward(mc_adjoint* adj, double* lambda, double* dgamma, void* stream);
 
+/* Tangent-linear (forward-mode) derivative of n_steps steps of the scheme the
+ * adjoint covers (2D, WENO5-Z + HLLC, FP64, periodic faces, any stepper),
+ * with dt = compute_dt under *clock each step: Q (device, ghosts filled or
+ * not) is advanced in place, bit-identical to the forward kernels, and dQ
+ * (device, n_dirs states in the layout of Q: on entry the tangents of the
+ * initial state, on exit those of the final state) together with dgamma
+ * (host, n_dirs values: the tangent of gamma in each direction) is carried
+ * along by dual-number evaluation of the forward arithmetic, each branch
+ * (WENO weights, HLLC wave speeds, min / max / |x|, the CFL arg-min cell)
+ * taken as the forward run takes it. dt's derivative is that of
+ * max_cfl * dx / (c_s + |v|) at the lowest-index cell holding the CFL
+ * minimum, zero when the output clamp fixes dt. Allocates its own scratch;
+ * waits for the stream; *clock returns advanced. An independent check of
+ * mc_adjoint_backward: <lambda, J dQ> computed both ways must agree. No
+ * counterpart in the reference. */
+mc_status mc_tangent_linear(const mc_grid* grid, const mc_scheme* scheme, double* Q, double* dQ,
+                            const double* dgamma, int32_t n_dirs, mc_clock* clock, int64_t n_steps, void* stream);
+
 /* One SSPRK step in place on Q, like mc_time_step, without a context and
  * without allocating any device memory. No counterpart in the reference.
  *

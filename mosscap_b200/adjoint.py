@@ -127,3 +127,47 @@ def kh_vy(problem: Problem) -> np.ndarray:
     ng = problem.ng
     q = problem.Q[:, 0, ng:-ng, ng:-ng]
     return q[2] / q[0]
+
+
+def tangent_linear(problem: Problem, q0: torch.Tensor, gamma: float, dq0: torch.Tensor, dgamma, n_steps: int):
+    """Forward-mode derivative of ``n_steps`` steps (``mc_tangent_linear``):
+    ``q0`` the interior state [4, ny, nx], ``dq0`` k tangent states
+    [k, 4, ny, nx], ``dgamma`` k tangents of gamma. Returns the final
+    interior state (bit-identical to ``EulerSteps``' forward run) and the k
+    final tangents [k, 4, ny, nx]."""
+    lib = capi.load()
+    ng = problem.ng
+    k = int(dq0.shape[0])
+    qpad = pad_periodic(q0.detach().to(torch.float64), ng)
+    dpad = torch.stack([pad_periodic(dq0[i].detach().to(torch.float64), ng) for i in range(k)]).contiguous()
+    grid = grid_of(problem)
+    scheme = _scheme(problem, gamma)
+    clk = capi.McClock()
+    clk.time, clk.max_time = 0.0, 1e300
+    clk.prev_output_time, clk.output_delta = 0.0, 1e300
+    dg = (ctypes.c_double * k)(*[float(x) for x in dgamma])
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    capi.check(lib.mc_tangent_linear(ctypes.byref(grid), ctypes.byref(scheme), ctypes.c_void_p(qpad.data_ptr()),
+                                     ctypes.c_void_p(dpad.data_ptr()), dg, k, ctypes.byref(clk), int(n_steps),
+                                     stream), "mc_tangent_linear")
+    return qpad[:, 0, ng:-ng, ng:-ng].clone(), dpad[:, :, 0, ng:-ng, ng:-ng].clone()
+
+
+def kh_directional_derivatives(problem: Problem, vy: torch.Tensor, gamma: float, dvy: torch.Tensor, dgamma,
+                               rho_target: torch.Tensor, n_steps: int):
+    """Directional derivatives of J = 1/2 |rho_final - rho_target|^2 along
+    the directions (dvy[k], dgamma[k]) of (initial vy field, gamma) by the
+    tangent-linear model: the initial tangents are the forward-mode
+    derivatives of kh_initial_state; returns (J, [dJ_k])."""
+    with torch.no_grad():
+        g = torch.tensor(gamma, dtype=torch.float64, device=vy.device)
+        q0 = kh_initial_state(vy, g, problem)
+        dq0 = []
+        for k in range(dvy.shape[0]):
+            tg = torch.tensor(float(dgamma[k]), dtype=torch.float64, device=vy.device)
+            dq0.append(torch.func.jvp(lambda v, gg: kh_initial_state(v, gg, problem), (vy, g), (dvy[k], tg))[1])
+        qn, dqn = tangent_linear(problem, q0, gamma, torch.stack(dq0), dgamma, n_steps)
+        r = qn[0] - rho_target
+        J = 0.5 * float((r * r).sum())
+        dJ = [float((r * dqn[k, 0]).sum()) for k in range(dqn.shape[0])]
+    return J, dJ

@@ -140,21 +140,23 @@ __device__ __forceinline__ void source_dt(const StageParams& p, int k, int j, in
 }
 
 // One SSPRK stage update of one variable; qu is the flux divergence already
-// multiplied by dt/dx and src the source term times dt.
-__device__ __forceinline__ double combine(int combo, double q_old, double q_in, double qu, double src) {
+// multiplied by dt/dx and src the source term times dt. T is double in the
+// stage kernels (and a dual number in the tangent-linear kernels).
+template <class T>
+__device__ __forceinline__ T combine(int combo, T q_old, T q_in, T qu, T src) {
     switch (combo) {
         case kAdd:
             return q_in + (qu + src);
         case kRk2Final:
-            return 0.5 * (q_old + q_in + qu + src);
+            return T(0.5) * (q_old + q_in + qu + src);
         case kSsp3Second:
-            return 0.75 * q_old + 0.25 * (q_in + qu + src);
+            return T(0.75) * q_old + T(0.25) * (q_in + qu + src);
         case kSsp3Final:
-            return (1.0 / 3.0) * q_old + (2.0 / 3.0) * (q_in + qu + src);
+            return T(1.0 / 3.0) * q_old + T(2.0 / 3.0) * (q_in + qu + src);
         case kHalfAdd:
-            return q_in + 0.5 * (qu + src);
+            return q_in + T(0.5) * (qu + src);
         default:
-            return (2.0 / 3.0) * q_old + (1.0 / 3.0) * q_in + (1.0 / 6.0) * (qu + src);
+            return T(2.0 / 3.0) * q_old + T(1.0 / 3.0) * q_in + T(1.0 / 6.0) * (qu + src);
     }
 }
 

@@ -44,16 +44,20 @@ class _CudaArray:
 
 
 def exchange_rows(q: torch.Tensor, ng: int, ny: int, rank: int, world: int, periodic: bool,
-                  group=None) -> None:
+                  group=None, via_host: bool = False) -> None:
     """Fill the y ghost rows of a slab from its neighbours.
 
     q: [nvar, 1, ny + 2 ng, xc] (this rank's slab with ghosts). Rows
     [ng, 2 ng) go to the rank below (its top ghosts), rows [ny, ny + ng) to
     the rank above (its bottom ghosts). Ranks 0 and world-1 exchange with each
     other only if the outer faces are periodic; otherwise their outer ghost
-    rows are left to the kernels' own boundary handling."""
+    rows are left to the kernels' own boundary handling. via_host: the rows
+    travel through host memory (for a process group whose backend moves
+    host tensors, e.g. gloo)."""
     lo_send = q[:, 0, ng:2 * ng, :].contiguous()
     hi_send = q[:, 0, ny:ny + ng, :].contiguous()
+    if via_host:
+        lo_send, hi_send = lo_send.cpu(), hi_send.cpu()
     below = rank - 1 if rank > 0 else (world - 1 if periodic else None)
     above = rank + 1 if rank < world - 1 else (0 if periodic else None)
     if world == 1:
@@ -82,9 +86,9 @@ def exchange_rows(q: torch.Tensor, ng: int, ny: int, rank: int, world: int, peri
         for r in dist.batch_isend_irecv(ops):
             r.wait()
     if below is not None:
-        q[:, 0, 0:ng, :] = lo_recv
+        q[:, 0, 0:ng, :] = lo_recv.to(q.device)
     if above is not None:
-        q[:, 0, ny + ng:ny + 2 * ng, :] = hi_recv
+        q[:, 0, ny + ng:ny + 2 * ng, :] = hi_recv.to(q.device)
 
 
 def clamp_to_output(dt: float, time: float, max_time: float, prev_output_time: float, delta: float) -> float:
@@ -102,11 +106,15 @@ class SlabSim:
     """This rank's slab of a 2D problem split along y over `world` ranks."""
 
     def __init__(self, problem: Problem, rank: int = 0, world: int = 1, precision: str = "fp64",
-                 device: Optional[torch.device] = None, group=None, is_slab: bool = False):
+                 device: Optional[torch.device] = None, group=None, is_slab: bool = False,
+                 via_host: bool = False):
         """problem: the global problem, whose rows are split over the ranks;
         or, with is_slab, this rank's slab itself (its ny rows and their
         ghost rows, the global problem's face kinds), so that no rank builds
-        the global state."""
+        the global state. via_host: ghost rows and the CFL minimum travel
+        through host memory (a gloo process group); otherwise they stay on
+        the device (NCCL)."""
+        self.via_host = via_host
         p = problem
         if p.num_dim != 2 or (not is_slab and p.ny % world != 0):
             raise ValueError("a 2D problem whose row count divides by the number of ranks")
@@ -142,12 +150,17 @@ class SlabSim:
 
     def _reduce_min(self, user, ptr, stream):
         word = torch.as_tensor(_CudaArray(ptr, (1,), "<i8"), device=self.sim.device)
-        dist.all_reduce(word, op=dist.ReduceOp.MIN, group=self.group)
+        if self.via_host:
+            h = word.cpu()
+            dist.all_reduce(h, op=dist.ReduceOp.MIN, group=self.group)
+            word.copy_(h)
+        else:
+            dist.all_reduce(word, op=dist.ReduceOp.MIN, group=self.group)
 
     def _fill_rows(self, user, qptr, stream):
         shape = tuple(self.sim.Q.shape)
         q = torch.as_tensor(_CudaArray(qptr, shape), device=self.sim.device)
-        exchange_rows(q, self.ng, self.ny, self.rank, self.world, self.periodic_y, self.group)
+        exchange_rows(q, self.ng, self.ny, self.rank, self.world, self.periodic_y, self.group, self.via_host)
 
     @property
     def time(self) -> float:
@@ -166,7 +179,7 @@ class SlabSim:
         else:
             local = self.sim.compute_dt(clamp=False)
         if self.world > 1:
-            t = torch.tensor([local], dtype=torch.float64, device=self.sim.device)
+            t = torch.tensor([local], dtype=torch.float64, device="cpu" if self.via_host else self.sim.device)
             dist.all_reduce(t, op=dist.ReduceOp.MIN, group=self.group)
             local = float(t.item())
         s = self.sim

@@ -132,3 +132,55 @@ def test_reverse_reciprocal_error_bound(gpu_lib):
     ref = 1.0 / x
     ulps = np.abs(out.cpu().numpy() - ref) / np.spacing(np.abs(ref))
     assert ulps.max() <= 2.0, ulps.max()
+
+
+def test_gpu_tangent_linear_matches_numpy_reference(gpu_lib):
+    """mc_tangent_linear (dual numbers through the forward kernels'
+    arithmetic) against the numpy tangent-linear model: two independent
+    forward-mode derivatives of the same discrete map."""
+    import tlm_reference as T
+    from mosscap_b200.adjoint import kh_directional_derivatives
+    n, steps = 24, 6
+    p, vy, pt = _setup(n, seed=4, target_seed=5)
+    rho_t = _target_rho(pt, p.gamma, steps)
+    rng = np.random.default_rng(9)
+    dirs = [rng.standard_normal((n, n)) for _ in range(3)]
+    dgs = [float(rng.standard_normal()) * 0.05 for _ in range(3)]
+    J, dJ = kh_directional_derivatives(p, vy, p.gamma, torch.tensor(np.stack(dirs), device="cuda"), dgs, rho_t,
+                                       steps)
+    for k in range(3):
+        tl, jref = T.directional_derivative(vy.cpu().numpy(), dirs[k], p.gamma, dgs[k], rho_t.cpu().numpy(), n,
+                                            p.max_cfl, steps)
+        assert abs(jref - J) / J < 1e-12, (jref, J)
+        assert abs(tl - dJ[k]) / abs(tl) < 1e-10, (k, tl, dJ[k])
+
+
+def test_gpu_tangent_linear_value_is_the_forward_state(gpu_lib):
+    from mosscap_b200.adjoint import EulerSteps, kh_initial_state, tangent_linear
+    n, steps = 40, 7
+    p, vy, _ = _setup(n, seed=3)
+    with torch.no_grad():
+        g = torch.tensor(p.gamma, dtype=torch.float64, device="cuda")
+        q0 = kh_initial_state(vy, g, p)
+        qf = EulerSteps.apply(q0, g, p, steps, 1000)
+        qt, _ = tangent_linear(p, q0, p.gamma, torch.zeros((1,) + tuple(q0.shape), dtype=torch.float64,
+                                                                device="cuda"), [0.0], steps)
+    assert torch.equal(qf, qt)
+
+
+def test_adjoint_matches_gpu_tangent_linear(gpu_lib):
+    """The reverse sweep against the tangent-linear model on 8 random
+    directions (64^2, 40 steps, checkpoints every 20)."""
+    from mosscap_b200.adjoint import kh_directional_derivatives
+    n, steps, ckpt = 64, 40, 20
+    p, vy, pt = _setup(n, seed=8, target_seed=9)
+    rho_t = _target_rho(pt, p.gamma, steps)
+    J, gvy, gg = _loss_and_grad(p, vy, p.gamma, rho_t, steps, ckpt)
+    rng = np.random.default_rng(10)
+    dirs = torch.tensor(rng.standard_normal((8, n, n)), device="cuda")
+    dgs = [float(x) * 1e-2 for x in rng.standard_normal(8)]
+    Jt, dJ = kh_directional_derivatives(p, vy, p.gamma, dirs, dgs, rho_t, steps)
+    assert abs(Jt - J) / J < 1e-13, (Jt, J)
+    for k in range(8):
+        ad = float((gvy * dirs[k]).sum()) + gg * dgs[k]
+        assert abs(ad - dJ[k]) / abs(dJ[k]) < 1e-9, (k, ad, dJ[k])
