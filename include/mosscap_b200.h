@@ -47,6 +47,7 @@ typedef enum {
 #define MC_FLAG_NEG_PRESSURE 0x4u  /* p <= 0 */
 #define MC_FLAG_BAD_DT 0x8u        /* dt <= 0 or not finite */
 #define MC_FLAG_EOS 0x10u          /* a non-ideal EOS update met a state the reference aborts on */
+#define MC_FLAG_TIMEOUT 0x20u      /* a kernel's bounded wait (a TMA tile copy) gave up; the tile was not updated */
 
 /* Enum values equal the reference's ordinals. */
 typedef enum { /* source/Reconstruct.hpp:10-15 */

@@ -6,6 +6,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "launch.h"
 #include "stage_kernels.cuh"
 
@@ -42,6 +44,39 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// The TMA tile load applies when the kernel has a TMA form for this
+// reconstruction and still fits its CTAs per SM, the tile's x start is even
+// (ng - H even), there are no tracers, and the stage input's tensor map can
+// be built (16-byte aligned base, even row length, box inside the array).
+template <int NDIM, int REC>
+bool use_tma(const StageParams& p, CUtensorMap* map) {
+    using G = TileGeom<2, REC>;
+    if (!tma_capable<NDIM, REC, Real>(p.nvar) || p.ntracer != 0 || ((p.ng - G::H) & 1) != 0) {
+        return false;
+    }
+    std::memset(map, 0, sizeof(*map));
+    return tma_map_for(p.q_in, p.xc, p.yc, p.zc, p.nvar, G::WX, G::WY, 2 + NDIM, map);
+}
+
+// The tiled kernel (2D stage, or the 3D x-y plane pass) with or without the
+// TMA tile load.
+template <int NDIM, int REC, int LIM, int RS, bool SRC, bool TMA>
+cudaError_t launch_tiled(const StageParams& p, const CUtensorMap& map, cudaStream_t s) {
+    if constexpr (TMA && !tma_capable<NDIM, REC, Real>(2 + NDIM)) {
+        return cudaErrorNotSupported;  // never taken: use_tma refused it
+    } else {
+        auto k = stage2d_kernel<NDIM, REC, LIM, RS, Real, SRC, TMA>;
+        const size_t sm = TMA ? smem_bytes_tma<NDIM, REC, Real>(p.nvar) : smem_bytes<NDIM, REC, Real>(p.nvar);
+        cudaError_t e = allow_smem(k, sm);
+        if (e != cudaSuccess) {
+            return e;
+        }
+        const dim3 grid(cdiv(p.nx, kTile), cdiv(p.ny, kTile), NDIM == 3 ? p.nz : 1);
+        k<<<grid, dim3(tile_threads<NDIM, Real>()), sm, s>>>(p, map);
+        return cudaGetLastError();
+    }
+}
+
 template <int REC, int LIM, int RS>
 cudaError_t launch_one(const StageParams& p, int pass, cudaStream_t s) {
 #if MC_DIM == 1
@@ -55,22 +90,19 @@ cudaError_t launch_one(const StageParams& p, int pass, cudaStream_t s) {
     k<<<dim3(cdiv(p.nx, kWarps * kTile)), dim3(kThreads), sm, s>>>(p);
 #elif MC_DIM == 2
     (void)pass;
-    auto k = stage2d_kernel<2, REC, LIM, RS, Real, MC_SRC>;
-    const size_t sm = smem_bytes<2, REC, Real>(p.nvar);
-    cudaError_t e = allow_smem(k, sm);
-    if (e != cudaSuccess) {
-        return e;
+    CUtensorMap map;
+    if (use_tma<2, REC>(p, &map)) {
+        return launch_tiled<2, REC, LIM, RS, MC_SRC, true>(p, map, s);
     }
-    k<<<dim3(cdiv(p.nx, kTile), cdiv(p.ny, kTile)), dim3(tile_threads<2, Real>()), sm, s>>>(p);
+    return launch_tiled<2, REC, LIM, RS, MC_SRC, false>(p, map, s);
 #else
     if (pass == 0) {
-        auto k = stage2d_kernel<3, REC, LIM, RS, Real>;
-        const size_t sm = smem_bytes<3, REC, Real>(p.nvar);
-        cudaError_t e = allow_smem(k, sm);
+        CUtensorMap map;
+        const cudaError_t e = use_tma<3, REC>(p, &map) ? launch_tiled<3, REC, LIM, RS, false, true>(p, map, s)
+                                                      : launch_tiled<3, REC, LIM, RS, false, false>(p, map, s);
         if (e != cudaSuccess) {
             return e;
         }
-        k<<<dim3(cdiv(p.nx, kTile), cdiv(p.ny, kTile), p.nz), dim3(tile_threads<3, Real>()), sm, s>>>(p);
     } else {
         auto k = ztile3d_kernel<REC, LIM, RS, Real, MC_SRC>;
         const size_t sm = ztile_smem_bytes<REC, Real>(p.nvar);

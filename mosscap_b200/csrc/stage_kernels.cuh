@@ -29,6 +29,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace mc {
 
@@ -68,6 +69,27 @@ __host__ __device__ constexpr int smem_dqy_per_var() {
 template <int NDIM, int REC, class T>
 __host__ __device__ constexpr size_t smem_bytes(int nvar) {
     return sizeof(T) * (size_t)nvar * (smem_w_per_var<NDIM, REC>() + smem_dqy_per_var<NDIM, REC>());
+}
+
+// Shared memory of the tiled kernels with a TMA tile load: a 128-byte
+// aligned region that first holds the conserved tile as the TMA copies it
+// (WY rows x WX cells x 2 + NDIM variables, doubles; corners included) and
+// later the y divergences (it is free once the tile is converted), then the
+// primitive tile W.
+template <int NDIM, int REC>
+__host__ __device__ constexpr size_t tma_stage_bytes() {
+    using G = TileGeom<2, REC>;
+    return sizeof(double) * (size_t)(2 + NDIM) * G::WY * G::WX;
+}
+template <int NDIM, int REC, class T>
+__host__ __device__ constexpr size_t tma_region_bytes(int nvar) {
+    const size_t dy = sizeof(T) * (size_t)nvar * smem_dqy_per_var<2, REC>();
+    const size_t st = tma_stage_bytes<NDIM, REC>();
+    return ((dy > st ? dy : st) + 127) / 128 * 128;
+}
+template <int NDIM, int REC, class T>
+__host__ __device__ constexpr size_t smem_bytes_tma(int nvar) {
+    return 128 + tma_region_bytes<NDIM, REC, T>(nvar) + sizeof(T) * (size_t)nvar * smem_w_per_var<2, REC>();
 }
 
 __device__ __forceinline__ long long qidx(const StageParams& p, int v, int k, int j, int i) {
@@ -232,6 +254,43 @@ __device__ __forceinline__ unsigned load_prim(const StageParams& p, int k, int j
             const double qt = inb ? p.q_in[id0 + (nh + t) * vs] : 0.0;
             w_smem[(nh + t) * var_stride] = T(qt * inv_rho);
         }
+    }
+    if (!inb) {
+        return 0u;
+    }
+    bool fin = true;
+#pragma unroll
+    for (int v = 0; v < nh; ++v) {
+        fin = fin && isfinite(q[v]);
+    }
+    return state_flags(w[0], w[nh - 1], fin);
+}
+
+// The same as load_prim for a cell whose conserved variables sit in the
+// TMA-staged tile (variable stride stg_vs doubles); no tracers.
+template <int NDIM, class T>
+__device__ __forceinline__ unsigned staged_prim(const StageParams& p, const double* src, int stg_vs, bool inb,
+                                                T* w_smem, int var_stride) {
+    constexpr int nh = 2 + NDIM;
+    double q[nh], w[nh];
+    if (inb) {
+#pragma unroll
+        for (int v = 0; v < nh; ++v) {
+            q[v] = src[v * stg_vs];
+        }
+    } else {
+        // outside the array: a benign state that no stored result depends on
+        q[0] = 1.0;
+#pragma unroll
+        for (int v = 1; v < nh - 1; ++v) {
+            q[v] = 0.0;
+        }
+        q[nh - 1] = 1.0;
+    }
+    prim_from_cons<NDIM>(p.gamma, q, w);
+#pragma unroll
+    for (int v = 0; v < nh; ++v) {
+        w_smem[v * var_stride] = T(w[v]);
     }
     if (!inb) {
         return 0u;
@@ -435,17 +494,29 @@ __global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
 // One CTA updates tile (bx, by) of a 2D problem, or of z plane bz in the 3D
 // plane pass. smem holds nvar x (WY x P) primitives and nvar x (TY x PY)
 // y divergences. Contains CTA-wide barriers: every thread of the CTA calls it.
-template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false, int NT = kThreads>
+//
+// TMA: smem is a 128-byte aligned region laid out as smem_bytes_tma
+// describes; the conserved tile arrives by one tensor copy (tmap, completed
+// on mbar) instead of per-thread loads. Without TMA, smem holds W and then
+// the y divergences (smem_bytes).
+template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false, int NT = kThreads, bool TMA = false>
 __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int bz, T* smem, double& dtmin,
-                                       unsigned& flags) {
+                                       unsigned& flags, const CUtensorMap* tmap = nullptr, uint64_t* mbar = nullptr) {
     constexpr int nh = 2 + NDIM;
     constexpr int NW = NT / 32;
     using G = TileGeom<2, REC>;
     constexpr int H = G::H, TX = G::TX, TY = G::TY, WX = G::WX, P = G::P, WY = G::WY, PY = G::PY;
     constexpr int WV = WY * P;   // per-variable stride of W
     constexpr int YV = TY * PY;  // per-variable stride of dFy
-    T* W = smem;
-    T* DY = W + (size_t)p.nvar * WV;
+    T* W;
+    T* DY;
+    if constexpr (TMA) {
+        DY = smem;
+        W = reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(smem) + tma_region_bytes<NDIM, REC, T>(p.nvar));
+    } else {
+        W = smem;
+        DY = W + (size_t)p.nvar * WV;
+    }
 
     const int x0 = bx * TX;
     const int y0 = by * TY;
@@ -456,21 +527,68 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
     // phase 1: primitives of the tile and its cross-shaped halo
     constexpr int core = TY * WX;
     constexpr int items = core + 2 * H * TX;
-    for (int it = threadIdx.x; it < items; it += NT) {
-        int tx, ty;
-        if (it < core) {
-            ty = it / WX;
-            tx = it - ty * WX - H;
-        } else {
-            const int r = it - core;
-            const int hr = r / TX;
-            tx = r - hr * TX;
-            ty = hr < H ? hr - H : TY + hr - H;
+    if constexpr (TMA) {
+        // the box of WX x WY cells around the tile (x start even: the host
+        // only takes this path when ng - H is even), all hydro variables;
+        // cells outside the array arrive as zeros and are replaced below
+        double* stg = reinterpret_cast<double*>(smem);
+        if (threadIdx.x == 0) {
+            mbar_init(mbar, 1);
         }
-        const int i = p.ng + x0 + tx;
-        const int j = p.ng + y0 + ty;
-        const bool inb = i >= 0 && i < p.xc && j >= 0 && j < p.yc;
-        flags |= load_prim<NDIM, T>(p, k, j, i, inb, W + (ty + H) * P + (tx + H), WV);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            mbar_expect_tx(mbar, (uint32_t)tma_stage_bytes<NDIM, REC>());
+            if constexpr (NDIM == 3) {
+                tma_load_4d(stg, tmap, p.ng + x0 - H, p.ng + y0 - H, k, 0, mbar);
+            } else {
+                tma_load_3d(stg, tmap, p.ng + x0 - H, p.ng + y0 - H, 0, mbar);
+            }
+        }
+        const bool ok = mbar_wait_bounded(mbar, 0, kTmaWaitPolls);
+        if (!__syncthreads_and(ok)) {
+            // the copy did not complete: raise the flag, give the copy in
+            // flight one more bounded wait, and leave the tile unwritten
+            if (threadIdx.x == 0) {
+                atomicOr(&p.blk->status, 0x20u);
+            }
+            mbar_wait_bounded(mbar, 0, kTmaWaitPolls);
+            __syncthreads();
+            return;
+        }
+        for (int it = threadIdx.x; it < items; it += NT) {
+            int tx, ty;
+            if (it < core) {
+                ty = it / WX;
+                tx = it - ty * WX - H;
+            } else {
+                const int r = it - core;
+                const int hr = r / TX;
+                tx = r - hr * TX;
+                ty = hr < H ? hr - H : TY + hr - H;
+            }
+            const int i = p.ng + x0 + tx;
+            const int j = p.ng + y0 + ty;
+            const bool inb = i >= 0 && i < p.xc && j >= 0 && j < p.yc;
+            flags |= staged_prim<NDIM, T>(p, stg + (ty + H) * WX + (tx + H), WX * WY, inb,
+                                          W + (ty + H) * P + (tx + H), WV);
+        }
+    } else {
+        for (int it = threadIdx.x; it < items; it += NT) {
+            int tx, ty;
+            if (it < core) {
+                ty = it / WX;
+                tx = it - ty * WX - H;
+            } else {
+                const int r = it - core;
+                const int hr = r / TX;
+                tx = r - hr * TX;
+                ty = hr < H ? hr - H : TY + hr - H;
+            }
+            const int i = p.ng + x0 + tx;
+            const int j = p.ng + y0 + ty;
+            const bool inb = i >= 0 && i < p.xc && j >= 0 && j < p.yc;
+            flags |= load_prim<NDIM, T>(p, k, j, i, inb, W + (ty + H) * P + (tx + H), WV);
+        }
     }
     __syncthreads();
 
@@ -591,9 +709,18 @@ __host__ __device__ constexpr int tile_min_blocks() {
     return NDIM == 1 ? (sizeof(T) == 4 ? kMinBlocks2dF32 : kMinBlocks2d) : (sizeof(T) == 4 ? 3 : 2);
 }
 
-template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false>
+// Whether the TMA tile load fits the kernel's CTAs per SM (shared memory
+// of one SM: 228 KB, 1 KB of it reserved per CTA) and its halo allows an
+// even x start with the usual ng (MUSCL's two-cell halo does not with ng = 3).
+template <int NDIM, int REC, class T>
+__host__ __device__ constexpr bool tma_capable(int nvar) {
+    return REC != kMuscl &&
+           (size_t)tile_min_blocks<NDIM, T>() * (smem_bytes_tma<NDIM, REC, T>(nvar) + 1024 + 256) <= 233472;
+}
+
+template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false, bool TMA = false>
 __global__ void __launch_bounds__(tile_threads<NDIM, T>(), tile_min_blocks<NDIM, T>())
-    stage2d_kernel(StageParams p) {
+    stage2d_kernel(StageParams p, const __grid_constant__ CUtensorMap tmap) {
     if (p.dt_dev && p.blk->done) {
         return;
     }
@@ -602,10 +729,16 @@ __global__ void __launch_bounds__(tile_threads<NDIM, T>(), tile_min_blocks<NDIM,
     constexpr int NT = tile_threads<NDIM, T>();
     __shared__ double red_d[NT / 32];
     __shared__ unsigned red_u[NT / 32];
+    __shared__ __align__(8) uint64_t mbar;
     double dtmin = __longlong_as_double(0x7ff0000000000000ll);
     unsigned flags = 0;
-    tile2d<NDIM, REC, LIM, RS, T, SRC, NT>(p, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<T*>(smem_raw), dtmin,
-                                  flags);
+    unsigned char* base = smem_raw;
+    if constexpr (TMA) {
+        // the tensor copy's destination: 128-byte aligned
+        base += (128u - (smem_addr(smem_raw) & 127u)) & 127u;
+    }
+    tile2d<NDIM, REC, LIM, RS, T, SRC, NT, TMA>(p, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<T*>(base),
+                                                dtmin, flags, &tmap, &mbar);
     block_publish(dtmin, flags, NDIM != 3 && p.last != 0, p.blk, red_d, red_u);
 }
 
