@@ -10,9 +10,9 @@ Prints one JSON line (rank 0). Metric: zone-updates/s = interior cells x
 steps / time. With --gpus N (one process per GPU under torchrun) the problem
 is a 2048 x 2048N stack of the KH layer split along y, 2048^2 cells per
 rank (weak scaling), in the device-driven loop: after every stage each rank
-exchanges its 3 edge rows with its neighbours (NCCL send/recv through the
-boundary hook) and every step's dt is the global CFL minimum (NCCL
-all-reduce MIN through the CFL reduce hook), all in-stream; --decomp
+exchanges its 3 edge rows with its neighbours and every step's dt is the
+global CFL minimum, both issued by the library in the stream (NCCL
+send/recv and all-reduce MIN, mc_set_slab_decomposition); --decomp
 replicas runs an independent 2048^2 problem per rank instead. The timed region is
 bracketed by a barrier and device synchronisation and the time is the
 maximum over ranks.
@@ -80,7 +80,7 @@ def config(n, precision, world, decomp="auto"):
         c["grid"] = f"{n}x{n * world} (KH layer stacked {world}x in y)"
         c["parallelism"] = (f"slab decomposition along y over {world} GPUs, device-driven loop: ghost-row exchange "
                             f"after every stage (NCCL send/recv) and global CFL minimum (NCCL all-reduce MIN) "
-                            f"in-stream through the library's hooks")
+                            f"issued by the library in the stream")
     elif world > 1:
         c["parallelism"] = f"independent {n}x{n} problems x{world}"
     return c
@@ -267,16 +267,16 @@ def run_ours(args):
         # one n x (n * world) periodic layer stack split along y: rank r owns
         # rows [r n, (r + 1) n), a unit-square copy of the KH layer (continuous
         # across slabs, since the layer is periodic in y); ghost rows come from
-        # the neighbours after every stage (NCCL point-to-point through the
-        # boundary hook) and dt is the global CFL minimum (all-reduce MIN)
+        # the neighbours after every stage and dt is the global CFL minimum,
+        # both by the library's own NCCL calls in the stream
         from mosscap_b200.distributed import SlabSim
-        slab = SlabSim(p, rank, world, precision=args.precision, device=dev, is_slab=True)
+        slab = SlabSim(p, rank, world, precision=args.precision, device=dev, is_slab=True, transport="library")
         sim = slab.sim
         slab.fill_bcs()
 
         def advance(k):
             # device-driven loop: ghost rows and the global CFL minimum are
-            # exchanged in-stream through the library's hooks
+            # exchanged in-stream by the library
             return len(slab.advance(k)) if k else 0
     else:
         sim = HydroSim(p, precision=args.precision, device=dev)
@@ -472,16 +472,48 @@ def measure_batch(problems, precision, steps, warmup):
 
 def run_batch(args):
     """Batched independent Riemann problems: 2048 1D (64..4096 cells) and 2048
-    2D quadrant problems (64^2..512^2), MUSCL / minmod, rk2, own dt each."""
+    2D quadrant problems (64^2..512^2), MUSCL / minmod, rk2, own dt each.
+    With N ranks the problems are split by cost (interior cells) over the
+    ranks, which share no data; the value is all ranks' zone updates over
+    the slowest rank's time (strong scaling: the batch is fixed)."""
+    import torch
     from mosscap_b200 import problems as P
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     half = max(args.problems // 2, 1)
     probs = P.riemann_batch(seed=0, n1d=half, n2d=half, riemann_solver=args.solver)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        from mosscap_b200.distributed import partition_by_cost
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        mine = partition_by_cost([p.interior_cells for p in probs], world)[rank]
+        probs = [probs[k] for k in mine]
+        dist.barrier()
     r = measure_batch(probs, args.precision, args.steps, args.warmup)
-    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+    if world > 1:
+        t = torch.tensor([r["ms_per_step"], r["value"] * r["ms_per_step"]], dtype=torch.float64, device="cuda")
+        tm = t[:1].clone()
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        # all ranks' updates per step over the slowest rank's step time
+        r["value"] = float(t[1].item()) / float(tm.item())
+        r["ms_per_step"] = float(tm.item())
+        r["problems"] = args.problems
+        dist.destroy_process_group()
+        if rank != 0:
+            return
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
             "dtype": r["dtype"], "data": "synthetic",
+            "scaling": "strong",
             "config": {"workload": f"riemann_batch_{half}x1d_{half}x2d_muscl_minmod_{args.solver}_rk2_{args.precision}",
-                       "problems": r["problems"], "interior_cells": r["interior_cells"], "schedule": r["schedule"]},
+                       "problems": r["problems"], "interior_cells": r["interior_cells"], "schedule": r["schedule"],
+                       "parallelism": "one GPU" if world == 1 else
+                       f"problems split by cost (interior cells) over {world} GPUs, no data exchange"},
             "problems_flagged": r["problems_flagged"]}
     print(json.dumps(line), flush=True)
 

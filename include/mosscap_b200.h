@@ -162,6 +162,25 @@ mc_status mc_set_user_bc(mc_ctx* ctx, void (*fn)(void* user, double* Q, void* st
 mc_status mc_set_cfl_reduce_hook(mc_ctx* ctx, void (*fn)(void* user, uint64_t* cfl_min_bits, void* stream),
                                  void* user);
 
+/* Slab decomposition over ranks (one GPU per rank). The problem is split
+ * along its slowest active axis (y in 2D, z in 3D) into one slab per rank;
+ * each rank creates its context for its own slab (its interior cells along
+ * that axis, with ghost layers, the global problem's face kinds) and then
+ * joins the decomposition with the id rank 0 obtained from mc_slab_unique_id
+ * and handed to every rank (through any host channel). From then on the
+ * library itself fills the ghost layers between neighbouring slabs after
+ * every stage and after mc_fill_bcs (NCCL send/receive of the bordering ng
+ * layers, in the stream), and reduces the CFL minimum over all ranks
+ * wherever it forms a dt (NCCL all-reduce MIN in the stream, exact because a
+ * minimum does not depend on order): every rank takes the same dt and the
+ * slabs together advance bit-identically to the single domain. Periodic
+ * outer faces of the slab axis make the last and the first rank neighbours.
+ * mc_set_slab_decomposition is collective (every rank calls it) and blocks
+ * until all have joined. NCCL (libnccl.so.2) is loaded when first needed.
+ * No counterpart in the reference, which runs one domain. */
+mc_status mc_slab_unique_id(uint8_t* id /* 128 bytes */);
+mc_status mc_set_slab_decomposition(mc_ctx* ctx, const uint8_t* id, int32_t rank, int32_t world);
+
 /* ---- Non-ideal equations of state --------------------------------------------
  *
  * The EOS kinds of the reference (EosType ordinals, source/Eos.hpp:16-21);

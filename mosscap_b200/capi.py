@@ -127,6 +127,10 @@ def load() -> ctypes.CDLL:
     lib.mc_advance.restype = i32
     lib.mc_last_cfl_min.argtypes = [vp, P(d), vp]
     lib.mc_last_cfl_min.restype = i32
+    lib.mc_slab_unique_id.argtypes = [ctypes.c_char_p]
+    lib.mc_slab_unique_id.restype = i32
+    lib.mc_set_slab_decomposition.argtypes = [vp, ctypes.c_char_p, i32, i32]
+    lib.mc_set_slab_decomposition.restype = i32
     lib.mc_tangent_linear.argtypes = [P(McGrid), P(McScheme), vp, vp, P(d), i32, P(McClock), i64, vp]
     lib.mc_tangent_linear.restype = i32
     lib.mc_get_status.argtypes = [vp, P(ctypes.c_uint32), vp]

@@ -14,6 +14,7 @@
 #include "eos.h"
 #include "launch.h"
 #include "mosscap_b200.h"
+#include "slab.h"
 
 using mc::StageParams;
 
@@ -37,6 +38,8 @@ struct mc_ctx {
     void* user_bc_data = nullptr;
     void (*cfl_hook)(void*, uint64_t*, void*) = nullptr;  // mc_set_cfl_reduce_hook
     void* cfl_hook_data = nullptr;
+    mc::SlabExchange* slab = nullptr;  // mc_set_slab_decomposition
+    int slab_faces = 0;                // faces whose ghosts the slab exchange fills
     int gravity = 0;              // mc_set_gravity
     double grav[3] = {0.0, 0.0, 0.0};
     // non-ideal EOS (mc_set_eos)
@@ -193,15 +196,29 @@ mc::EosLaunch eos_launch(const mc_ctx* c, const double* q_in, double* q_out, boo
     return L;
 }
 
-// Faces of kind MC_BC_USERFN among the active ones (bit f = face f).
+// Faces of kind MC_BC_USERFN among the active ones (bit f = face f) whose
+// ghosts the caller's hook fills (not the slab exchange).
 int user_face_mask(const mc_ctx* c) {
     int m = 0;
     for (int f = 0; f < 2 * c->grid.num_dim; ++f) {
-        if (c->grid.bc[f] == MC_BC_USERFN) {
+        if (c->grid.bc[f] == MC_BC_USERFN && !((c->slab_faces >> f) & 1)) {
             m |= 1 << f;
         }
     }
     return m;
+}
+
+// The slab exchange of Q's ghost layers, if the context is one slab of a
+// decomposed problem.
+mc_status exchange_slab(mc_ctx* c, double* q, cudaStream_t s) {
+    if (!c->slab) {
+        return MC_OK;
+    }
+    const char* why = "";
+    if (mc::slab_exchange(c->slab, q, s, &why) != cudaSuccess) {
+        return fail(MC_ERR_CUDA, std::string("slab exchange: ") + why);
+    }
+    return MC_OK;
 }
 
 // Enqueue one SSPRK step on Q. dt_dev (device-driven loop) or dt (host).
@@ -239,6 +256,9 @@ mc_status enqueue_step(mc_ctx* c, double* Q, double dt, const double* dt_dev, bo
             p.reset_min = 0;
             MC_CUDA(launch_stage(c, p, 1, s), "stage launch (z pass)");
         }
+        if (mc_status st = exchange_slab(c, p.q_out, s)) {
+            return st;
+        }
         if (c->user_bc) {
             c->user_bc(c->user_bc_data, p.q_out, (void*)s);
             // the hook fills the MC_BC_USERFN ghosts after the fused CFL
@@ -255,11 +275,20 @@ mc_status enqueue_step(mc_ctx* c, double* Q, double dt, const double* dt_dev, bo
     return MC_OK;
 }
 
-// The caller's domain-wide reduction of the CFL minimum word, if any.
-void reduce_cfl(mc_ctx* c, cudaStream_t s) {
-    if (c->cfl_hook) {
-        c->cfl_hook(c->cfl_hook_data, reinterpret_cast<uint64_t*>(&c->blk->cfl_min_bits), (void*)s);
+// The domain-wide reduction of the CFL minimum word: the slab
+// decomposition's all-reduce and the caller's hook, if any.
+mc_status reduce_cfl(mc_ctx* c, cudaStream_t s) {
+    uint64_t* word = reinterpret_cast<uint64_t*>(&c->blk->cfl_min_bits);
+    if (c->slab) {
+        const char* why = "";
+        if (mc::slab_reduce_min(c->slab, word, s, &why) != cudaSuccess) {
+            return fail(MC_ERR_CUDA, std::string("slab CFL all-reduce: ") + why);
+        }
     }
+    if (c->cfl_hook) {
+        c->cfl_hook(c->cfl_hook_data, word, (void*)s);
+    }
+    return MC_OK;
 }
 
 double clamp_to_output(double dt, const mc_clock* k) {
@@ -282,10 +311,11 @@ mc_status check_ctx(const mc_ctx* c) {
     return MC_OK;
 }
 
-// A MC_BC_USERFN face is filled only by the caller's hook.
+// A MC_BC_USERFN face is filled only by the caller's hook (or the slab
+// exchange).
 mc_status check_user_bc(const mc_ctx* c) {
     for (int f = 0; f < 2 * c->grid.num_dim; ++f) {
-        if (c->grid.bc[f] == MC_BC_USERFN && !c->user_bc) {
+        if (c->grid.bc[f] == MC_BC_USERFN && !((c->slab_faces >> f) & 1) && !c->user_bc) {
             return fail(MC_ERR_INVALID_ARGUMENT, "a MC_BC_USERFN face needs mc_set_user_bc");
         }
     }
@@ -403,6 +433,7 @@ mc_status mc_destroy(mc_ctx* c) {
     if (!c) {
         return MC_OK;
     }
+    mc::slab_destroy(c->slab);
     cudaFree(c->buf_a);
     cudaFree(c->buf_b);
     cudaFree(c->dqxy);
@@ -444,6 +475,54 @@ mc_status mc_set_gravity(mc_ctx* c, int32_t enabled, double gx, double gy, doubl
     c->grav[0] = enabled ? gx : 0.0;
     c->grav[1] = enabled && c->grid.num_dim > 1 ? gy : 0.0;
     c->grav[2] = enabled && c->grid.num_dim > 2 ? gz : 0.0;
+    return MC_OK;
+}
+
+mc_status mc_slab_unique_id(uint8_t* id) {
+    if (!id) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null id");
+    }
+    const char* why = "";
+    if (!mc::slab_unique_id(id, &why)) {
+        return fail(MC_ERR_UNSUPPORTED, std::string("mc_slab_unique_id: ") + why);
+    }
+    return MC_OK;
+}
+
+mc_status mc_set_slab_decomposition(mc_ctx* c, const uint8_t* id, int32_t rank, int32_t world) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    if (!id || world < 1 || rank < 0 || rank >= world) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null id or rank outside [0, world)");
+    }
+    if (c->grid.num_dim < 2) {
+        return fail(MC_ERR_UNSUPPORTED, "slab decomposition splits y (2D) or z (3D)");
+    }
+    if (c->slab) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "the context already holds a slab decomposition");
+    }
+    const int axis = c->grid.num_dim - 1;
+    const int f0 = 2 * axis;
+    if ((c->grid.bc[f0] == MC_BC_PERIODIC) != (c->grid.bc[f0 + 1] == MC_BC_PERIODIC)) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "periodic boundaries come in pairs");
+    }
+    const bool periodic = c->grid.bc[f0] == MC_BC_PERIODIC;
+    const int n = axis == 1 ? c->ny : c->nz;
+    const char* why = "";
+    mc::SlabExchange* s = mc::slab_create(id, rank, world, axis, n, c->grid.ng, c->grid.xc, c->grid.yc,
+                                          c->grid.zc, c->nvar, periodic, &why);
+    if (!s) {
+        return fail(MC_ERR_CUDA, std::string("slab communicator: ") + why);
+    }
+    c->slab = s;
+    c->slab_faces = mc::slab_face_mask(s);
+    // the kernels leave the exchanged faces' ghosts alone
+    for (int f = f0; f < f0 + 2; ++f) {
+        if ((c->slab_faces >> f) & 1) {
+            c->grid.bc[f] = MC_BC_USERFN;
+        }
+    }
     return MC_OK;
 }
 
@@ -567,6 +646,9 @@ mc_status mc_fill_bcs(mc_ctx* c, double* Q, void* stream) {
     p.q_out = Q;
     c->launches += 1;
     MC_CUDA(mc::launch_fill_bcs(p, c->grid.num_dim, (cudaStream_t)stream), "fill_bcs");
+    if (mc_status st = exchange_slab(c, Q, (cudaStream_t)stream)) {
+        return st;
+    }
     if (c->user_bc) {
         c->user_bc(c->user_bc_data, Q, stream);
     }
@@ -585,7 +667,9 @@ mc_status mc_compute_dt(mc_ctx* c, const double* Q, const mc_clock* clock, doubl
     p.q_in = Q;
     c->launches += 2;
     MC_CUDA(mc::launch_cfl_min(p, c->grid.num_dim, s), "cfl_min");
-    reduce_cfl(c, s);
+    if (mc_status st = reduce_cfl(c, s)) {
+        return st;
+    }
     MC_CUDA(cudaMemcpyAsync(c->blk_host, c->blk, sizeof(mc::DeviceBlock), cudaMemcpyDeviceToHost, s), "read-back");
     MC_CUDA(cudaStreamSynchronize(s), "sync");
     double m;
@@ -642,7 +726,9 @@ mc_status mc_advance(mc_ctx* c, double* Q, mc_clock* clock, int64_t max_steps, i
     StageParams p = base_params(c);
     p.q_in = Q;
     MC_CUDA(mc::launch_cfl_min(p, c->grid.num_dim, s), "cfl_min");
-    reduce_cfl(c, s);
+    if (mc_status st = reduce_cfl(c, s)) {
+        return st;
+    }
     MC_CUDA(mc::launch_clock_advance(c->blk, dlog, 1, s), "clock");
     c->launches += 4;
     const double* dt_dev = &c->blk->dt;
@@ -654,7 +740,9 @@ mc_status mc_advance(mc_ctx* c, double* Q, mc_clock* clock, int64_t max_steps, i
             if (mc_status st = enqueue_step(c, Q, 0.0, dt_dev, false, s)) {
                 return st;
             }
-            reduce_cfl(c, s);
+            if (mc_status st = reduce_cfl(c, s)) {
+                return st;
+            }
             MC_CUDA(mc::launch_clock_advance(c->blk, dlog, 0, s), "clock");
             c->launches += 1;
         }

@@ -110,3 +110,20 @@ def test_cfl_minimum_by_integer_min_of_bits():
         p.join(timeout=120)
         assert p.exitcode == 0
     assert errors.empty(), errors.get()
+
+
+@pytest.mark.parametrize("world", [2, 3, 8])
+def test_partition_by_cost_balances_the_batch(world):
+    """The seeded 4096-problem batch split over ranks by interior cells:
+    every problem on exactly one rank, and the largest load within the
+    greedy rule's bound (mean load plus the largest problem)."""
+    from mosscap_b200 import problems as P
+    from mosscap_b200.distributed import partition_by_cost
+    probs = P.riemann_batch(seed=0, n1d=256, n2d=256)
+    costs = [p.interior_cells for p in probs]
+    parts = partition_by_cost(costs, world)
+    flat = sorted(k for part in parts for k in part)
+    assert flat == list(range(len(probs)))
+    loads = [sum(costs[k] for k in part) for part in parts]
+    assert max(loads) <= sum(costs) / world + max(costs)
+    assert max(loads) / (sum(costs) / world) < 1.02

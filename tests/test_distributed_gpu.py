@@ -42,7 +42,7 @@ def _worker(rank, world, port, loop, out_dir, errors):
     try:
         torch.cuda.set_device(0)
         p = P.kelvin_helmholtz_2d(N, seed=3)
-        slab = SlabSim(p, rank, world, device=torch.device("cuda", 0), via_host=True)
+        slab = SlabSim(p, rank, world, device=torch.device("cuda", 0), transport="host")
         slab.fill_bcs()
         if loop == "host":
             dts = np.array([slab.step() for _ in range(STEPS)])

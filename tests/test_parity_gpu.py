@@ -186,14 +186,18 @@ def test_fp32_form_error_bounds(gpu_lib, oracle_port):
     assert sim.status() == 0
 
 
-def test_slab_decomposition_device_loop_single_rank(gpu_lib, oracle_port):
+@pytest.mark.parametrize("transport", ["hook", "library"])
+def test_slab_decomposition_device_loop_single_rank(gpu_lib, oracle_port, transport):
     """The slab path in the device-driven loop (SlabSim.advance) on one rank
-    is bit-identical to the reference run of the same periodic problem."""
+    is bit-identical to the reference run of the same periodic problem: the
+    Python boundary hook, and the library's own NCCL exchange (one rank
+    sending its periodic ghost rows to itself) with the NCCL all-reduce of
+    the CFL minimum."""
     from mosscap_b200.distributed import SlabSim
     p = P.kelvin_helmholtz_2d(96, seed=6)
     o = _oracle(oracle_port, p)
     ref_dts = o.run(8)
-    s = SlabSim(p, rank=0, world=1)
+    s = SlabSim(p, rank=0, world=1, transport=transport)
     s.fill_bcs()
     dts = s.advance(8)
     _assert_same(np.array(dts), ref_dts, "dt")
@@ -242,15 +246,16 @@ def test_cfl_reduce_hook(gpu_lib):
     capi.check(sim2.lib.mc_set_cfl_reduce_hook(sim2.ctx, capi.CFL_REDUCE_FN(0), None), "unhook")
 
 
-def test_slab_decomposition_single_rank(gpu_lib, oracle_port):
-    """The slab path (y faces filled by the boundary hook, dt from the
-    step's fused CFL minimum) on one rank with a self-periodic exchange is
-    bit-identical to the reference run of the same periodic problem."""
+@pytest.mark.parametrize("transport", ["hook", "library"])
+def test_slab_decomposition_single_rank(gpu_lib, oracle_port, transport):
+    """The slab path (y faces filled by the boundary hook or the library's
+    exchange, the host-driven loop) on one rank with a self-periodic exchange
+    is bit-identical to the reference run of the same periodic problem."""
     from mosscap_b200.distributed import SlabSim
     p = P.kelvin_helmholtz_2d(96, seed=5)
     o = _oracle(oracle_port, p)
     ref_dts = o.run(8)
-    s = SlabSim(p, rank=0, world=1)
+    s = SlabSim(p, rank=0, world=1, transport=transport)
     s.fill_bcs()
     dts = [s.step() for _ in range(8)]
     _assert_same(np.array(dts), ref_dts, "dt")
@@ -356,3 +361,24 @@ def test_tma_tile_path_tile_unaligned(gpu_lib, oracle_port, ndim, nx, ny, nz, re
         _assert_same(dts, ref_dts, f"dt ({loop})")
         _assert_same(sim.get_Q(), o.get_Q(), f"state ({loop})")
         assert sim.status() == 0
+
+
+@pytest.mark.parametrize("loop", ["host", "device"])
+def test_z_slab_decomposition_single_rank(gpu_lib, oracle_port, loop):
+    """A 3D z slab (PPM + HLL, periodic in z, walls and zero-gradient
+    elsewhere) through the library's NCCL exchange of ghost planes, one rank
+    sending its periodic planes to itself: bit-identical to the oracle."""
+    from mosscap_b200.distributed import SlabSim
+    nx, ny, nz = 40, 34, 36
+    q = P.random_state(3, nx, ny, nz, ng=3, seed=123)
+    p = P.Problem("zslab", 3, nx, ny, nz, ng=3, dx=1.0 / nz,
+                  bc=("wall", "zerograd", "symmetric", "wall", "periodic", "periodic"),
+                  reconstruction="ppm", slope_limiter="monotonizedcentral", riemann_solver="hll",
+                  time_stepper="ssprk3", gamma=1.4, max_cfl=0.3, max_time=1.0, output_delta=0.02, Q=q)
+    o = _oracle(oracle_port, p)
+    ref_dts = o.run(6)
+    s = SlabSim(p, rank=0, world=1, transport="library")
+    s.fill_bcs()
+    dts = [s.step() for _ in range(6)] if loop == "host" else s.advance(6)
+    _assert_same(np.array(dts), ref_dts, "dt")
+    _assert_same(s.sim.get_Q(), o.get_Q(), "state")
