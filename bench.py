@@ -62,6 +62,7 @@ def parse():
                          "or an independent problem per GPU (replicas)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="batch workload: keep the default schedule (no autotuner)")
     ap.add_argument("--no-extras", action="store_true",
                     help="kh2d at N=1: skip the FP32 form, Sedov 512^3, batch and adjoint measurements "
                          "that the default run adds to the line under 'forms'")
@@ -439,7 +440,7 @@ def run_sedov(args):
     print(json.dumps(line), flush=True)
 
 
-def measure_batch(problems, precision, steps, warmup):
+def measure_batch(problems, precision, steps, warmup, tune=True):
     """Batched independent problems (one persistent launch per stage kind,
     graph-replayed steps, autotuned schedule); returns a dict."""
     import torch
@@ -448,7 +449,7 @@ def measure_batch(problems, precision, steps, warmup):
     b = BatchSim(problems, precision=precision)
     b.fill_bcs()
     t0 = time.perf_counter()
-    sched = b.tune()
+    sched = b.tune() if tune else b.schedule()
     tune_s = time.perf_counter() - t0
     b.advance(warmup)
     _, k0, _ = b.clocks()
@@ -493,7 +494,7 @@ def run_batch(args):
         mine = partition_by_cost([p.interior_cells for p in probs], world)[rank]
         probs = [probs[k] for k in mine]
         dist.barrier()
-    r = measure_batch(probs, args.precision, args.steps, args.warmup)
+    r = measure_batch(probs, args.precision, args.steps, args.warmup, tune=not args.no_tune)
     if world > 1:
         t = torch.tensor([r["ms_per_step"], r["value"] * r["ms_per_step"]], dtype=torch.float64, device="cuda")
         tm = t[:1].clone()

@@ -220,6 +220,35 @@ __device__ __forceinline__ double write_cell(const StageParams& p, int i, int j,
     return dtmin;
 }
 
+// Primitives of a cell for the sweep of compute type T. T = double: the
+// reference's cons_to_prim (Eos.hpp:61-79), bit for bit. T = float (the FP32
+// compute form, whose sweep rounds to FP32 anyway): 1 / rho is formed once
+// in FP64, the velocities are m / rho through it, and the pressure is
+// recovered in FP64 from the total energy with the kinetic energy
+// |m|^2 / (2 rho), so that the cancellation E - e_kin of high-Mach and
+// near-vacuum cells stays an FP64 operation -- one FP64 division per cell
+// instead of 2 + (NDIM > 1) + (NDIM > 2).
+template <int NDIM, class T>
+__device__ __forceinline__ void prim_for_sweep(double gamma, const double* q, double* w) {
+    if constexpr (sizeof(T) == 8) {
+        prim_from_cons<NDIM>(gamma, q, w);
+    } else {
+        const double inv = 1.0 / q[0];
+        double m2 = q[1] * q[1];
+        w[0] = q[0];
+        w[1] = q[1] * inv;
+        if constexpr (NDIM > 1) {
+            m2 += q[2] * q[2];
+            w[2] = q[2] * inv;
+        }
+        if constexpr (NDIM > 2) {
+            m2 += q[3] * q[3];
+            w[3] = q[3] * inv;
+        }
+        w[1 + NDIM] = (gamma - 1.0) * (q[1 + NDIM] - 0.5 * m2 * inv);
+    }
+}
+
 // Load one cell's conserved variables from q_in and store its primitives
 // (tracers divided by rho, source/Hydro.cpp:27-33) into shared memory.
 template <int NDIM, class T>
@@ -243,7 +272,7 @@ __device__ __forceinline__ unsigned load_prim(const StageParams& p, int k, int j
         }
         q[nh - 1] = 1.0;
     }
-    prim_from_cons<NDIM>(p.gamma, q, w);
+    prim_for_sweep<NDIM, T>(p.gamma, q, w);
 #pragma unroll
     for (int v = 0; v < nh; ++v) {
         w_smem[v * var_stride] = T(w[v]);
@@ -287,7 +316,7 @@ __device__ __forceinline__ unsigned staged_prim(const StageParams& p, const doub
         }
         q[nh - 1] = 1.0;
     }
-    prim_from_cons<NDIM>(p.gamma, q, w);
+    prim_for_sweep<NDIM, T>(p.gamma, q, w);
 #pragma unroll
     for (int v = 0; v < nh; ++v) {
         w_smem[v * var_stride] = T(w[v]);
@@ -674,13 +703,18 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
                     qu[v] *= dtdx;
                 }
                 combine_all<nh>(p.combo, qo, qi, qu, sdt, qn);
-                for (int t = 0; t < ntr; ++t) {
-                    double qt = 0.0;
-                    qt += double(d_tr[t]);
-                    qt += double(dfy[(nh + t) * YV]);
-                    qt *= dtdx;
-                    const long long id = id0 + (nh + t) * vs;
-                    qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qt, 0.0);
+                // constant tracer slots keep qn in registers (a loop up to
+                // ntr would index it at run time and put it in local memory)
+#pragma unroll
+                for (int t = 0; t < kMaxVars - nh; ++t) {
+                    if (t < ntr) {
+                        double qt = 0.0;
+                        qt += double(d_tr[t]);
+                        qt += double(dfy[(nh + t) * YV]);
+                        qt *= dtdx;
+                        const long long id = id0 + (nh + t) * vs;
+                        qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qt, 0.0);
+                    }
                 }
                 dtmin = smin(write_cell<NDIM>(p, i, j, 0, qn, p.last != 0, &flags), dtmin);
             }
@@ -773,9 +807,10 @@ __host__ __device__ constexpr size_t ztile_smem_bytes(int nvar) {
 // integrate_flux (source/TimeStepping.cpp:22-27), the stage combination, the
 // store and the ghost scatter. Grid: (z chunks, x tiles, y rows), z chunks
 // fastest, so the halo rows a neighbouring chunk re-reads are still in L2.
+// Three CTAs per SM in both precisions: at four (64 registers) the FP32 z
+// pass spilled 196 bytes per thread.
 template <int REC, int LIM, int RS, class T, bool SRC = false>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? kMinBlocks2dF32 : kMinBlocks2d)
-    ztile3d_kernel(StageParams p) {
+__global__ void __launch_bounds__(kThreads, kMinBlocks2d) ztile3d_kernel(StageParams p) {
     if (p.dt_dev && p.blk->done) {
         return;
     }
