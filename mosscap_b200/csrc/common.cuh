@@ -267,6 +267,61 @@ __device__ __forceinline__ int axis_targets(int c, int n, int ng, int bs, int be
     return cnt;
 }
 
+// The same targets one at a time, without arrays (so that a kernel keeps
+// them in registers): the number of targets of index c (entry 0 is c
+// itself) and target k with its face (-1 for c itself, 0 start, 1 end), in
+// the order axis_targets lists them.
+__device__ __forceinline__ int start_target_count(int c, int n, int ng, int bs) {
+    if (bs == kPeriodic) {
+        return (c >= n && c < n + ng) ? 1 : 0;
+    }
+    if (bs == kWall || bs == kSymmetric || bs == kDiode) {
+        return (c >= ng && c < 2 * ng) ? 1 : 0;
+    }
+    if (bs == kZeroGrad || bs == kConstant) {
+        return c == ng ? ng : 0;
+    }
+    return 0;
+}
+__device__ __forceinline__ int end_target_count(int c, int n, int ng, int be) {
+    if (be == kPeriodic) {
+        return (c >= ng && c < 2 * ng) ? 1 : 0;
+    }
+    if (be == kWall || be == kSymmetric || be == kDiode) {
+        return (c >= n && c < n + ng) ? 1 : 0;
+    }
+    if (be == kZeroGrad || be == kConstant) {
+        return c == ng + n - 1 ? ng : 0;
+    }
+    return 0;
+}
+__device__ __forceinline__ int axis_target_at(int c, int n, int ng, int bs, int be, int ns, int k, int* face) {
+    if (k == 0) {
+        *face = -1;
+        return c;
+    }
+    k -= 1;
+    if (k < ns) {
+        *face = 0;
+        if (bs == kPeriodic) {
+            return c - n;
+        }
+        if (bs == kZeroGrad || bs == kConstant) {
+            return k;
+        }
+        return 2 * ng - 1 - c;
+    }
+    k -= ns;
+    *face = 1;
+    if (be == kPeriodic) {
+        return c + n;
+    }
+    if (be == kZeroGrad || be == kConstant) {
+        return ng + n + k;
+    }
+    return 2 * (ng + n) - 1 - c;
+}
+
 // Whether array index c along an axis feeds any ghost (fast-path test).
 __device__ __forceinline__ bool near_face(int c, int n, int ng) {
     return c < 2 * ng || c >= n;

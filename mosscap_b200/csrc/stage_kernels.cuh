@@ -96,27 +96,53 @@ __device__ __forceinline__ long long qidx(const StageParams& p, int v, int k, in
     return (((long long)v * p.zc + k) * p.yc + j) * (long long)p.xc + i;
 }
 
+// CFL time-step bound and status flags of one written conserved state.
+// FP64 path (T = double): the reference's dt_reducer (source/Hydro.cpp:
+// 192-206) from cons_to_prim, bit for bit. FP32 form (T = float): the same
+// bound in FP64 arithmetic from 1 / rho formed once (two FP64 divisions
+// instead of five in 3D): p = (gamma - 1)(E - |m|^2 / 2 rho),
+// c_s = sqrt(gamma p / rho), |v| = |m| / rho.
+template <int NDIM, class T>
+__device__ __forceinline__ double cfl_bound_of(const StageParams& p, const double* q, unsigned* flags) {
+    constexpr int nh = 2 + NDIM;
+    bool fin = true;
+#pragma unroll
+    for (int v = 0; v < nh; ++v) {
+        fin = fin && isfinite(q[v]);
+    }
+    if constexpr (sizeof(T) == 8) {
+        double w[nh];
+        prim_from_cons<NDIM>(p.gamma, q, w);
+        *flags |= state_flags(w[0], w[nh - 1], fin);
+        return cfl_dt<NDIM>(p.gamma, p.dx, w);
+    } else {
+        const double inv = 1.0 / q[0];
+        double m2 = q[1] * q[1];
+        if constexpr (NDIM > 1) {
+            m2 += q[2] * q[2];
+        }
+        if constexpr (NDIM > 2) {
+            m2 += q[3] * q[3];
+        }
+        const double pr = (p.gamma - 1.0) * (q[1 + NDIM] - 0.5 * m2 * inv);
+        *flags |= state_flags(q[0], pr, fin);
+        const double cs = sqrt(p.gamma * pr * inv);
+        return p.dx / (cs + sqrt(m2) * inv);
+    }
+}
+
 // Write the new value of interior cell (i, j, k) and every ghost it is the
 // source of; returns the CFL minimum over the written values (last stage) and
-// ORs their status flags into *flags.
-template <int NDIM>
+// ORs their status flags into *flags. The ghost targets along each axis are
+// enumerated one at a time (axis_target_at), so nothing goes to local memory.
+template <int NDIM, class T = double>
 __device__ __forceinline__ double write_cell(const StageParams& p, int i, int j, int k, double* qn,
                                              bool want_dt, unsigned* flags) {
-    constexpr int nh = 2 + NDIM;
     const int nvar = p.nvar;
     double dtmin = __longlong_as_double(0x7ff0000000000000ll);
     auto account = [&](const double* q) {
         if (want_dt) {
-            double w[nh];
-            prim_from_cons<NDIM>(p.gamma, q, w);
-            bool fin = true;
-#pragma unroll
-            for (int v = 0; v < nh; ++v) {
-                fin = fin && isfinite(q[v]);
-            }
-            *flags |= state_flags(w[0], w[nh - 1], fin);
-            const double d = cfl_dt<NDIM>(p.gamma, p.dx, w);
-            dtmin = smin(d, dtmin);
+            dtmin = smin(cfl_bound_of<NDIM, T>(p, q, flags), dtmin);
         }
     };
     const long long vs = (long long)p.zc * p.yc * p.xc;  // variable stride of the state
@@ -136,81 +162,51 @@ __device__ __forceinline__ double write_cell(const StageParams& p, int i, int j,
     if (!(nx_ || ny_ || nz_)) {
         return dtmin;
     }
-    int ix[2 * kMaxGhost + 1], fx[2 * kMaxGhost + 1];
-    int iy[2 * kMaxGhost + 1], fy[2 * kMaxGhost + 1];
-    int iz[2 * kMaxGhost + 1], fz[2 * kMaxGhost + 1];
-    const int cx = axis_targets(i, p.nx, p.ng, p.bc.kind[0], p.bc.kind[1], ix, fx);
-    int cy = 1, cz = 1;
-    iy[0] = j;
-    fy[0] = -1;
-    iz[0] = k;
-    fz[0] = -1;
+    const int sx = start_target_count(i, p.nx, p.ng, p.bc.kind[0]);
+    const int cx = 1 + sx + end_target_count(i, p.nx, p.ng, p.bc.kind[1]);
+    int sy = 0, cy = 1, sz = 0, cz = 1;
     if constexpr (NDIM > 1) {
-        cy = axis_targets(j, p.ny, p.ng, p.bc.kind[2], p.bc.kind[3], iy, fy);
+        sy = start_target_count(j, p.ny, p.ng, p.bc.kind[2]);
+        cy = 1 + sy + end_target_count(j, p.ny, p.ng, p.bc.kind[3]);
     }
     if constexpr (NDIM > 2) {
-        cz = axis_targets(k, p.nz, p.ng, p.bc.kind[4], p.bc.kind[5], iz, fz);
+        sz = start_target_count(k, p.nz, p.ng, p.bc.kind[4]);
+        cz = 1 + sz + end_target_count(k, p.nz, p.ng, p.bc.kind[5]);
     }
-    if constexpr (NDIM < 3) {
-        for (int a = 0; a < cx; ++a) {
-            double qa[kMaxVars];
-#pragma unroll
-            for (int v = 0; v < kMaxVars; ++v) {
-                qa[v] = qn[v];
-            }
-            if (fx[a] >= 0) {
-                bc_transform<NDIM>(p.bc, 0, fx[a], nvar, qa);
-            }
-            for (int b = 0; b < cy; ++b) {
-                if (a == 0 && b == 0) {
-                    continue;
-                }
-                double qb[kMaxVars];
-#pragma unroll
-                for (int v = 0; v < kMaxVars; ++v) {
-                    qb[v] = qa[v];
-                }
-                if (fy[b] >= 0) {
-                    bc_transform<NDIM>(p.bc, 1, fy[b], nvar, qb);
-                }
-#pragma unroll
-                for (int v = 0; v < kMaxVars; ++v) {
-                    if (v < nvar) {
-                        p.q_out[qidx(p, v, k, iy[b], ix[a])] = qb[v];
-                    }
-                }
-                account(qb);
-            }
-        }
-        return dtmin;
-    }
-    // 3D: each ghost target starts again from the cell's new state and
-    // applies the face transforms of its axes in x, y, z order, as the
-    // sequential per-axis fill does; only two states are live at a time
+    // each ghost target starts again from the cell's new state and applies
+    // the face transforms of its axes in x, y, z order, as the sequential
+    // per-axis fill does; only two states are live at a time
     for (int a = 0; a < cx; ++a) {
+        int fa;
+        const int ia = axis_target_at(i, p.nx, p.ng, p.bc.kind[0], p.bc.kind[1], sx, a, &fa);
         for (int b = 0; b < cy; ++b) {
+            int fb = -1;
+            const int jb = NDIM > 1 ? axis_target_at(j, p.ny, p.ng, p.bc.kind[2], p.bc.kind[3], sy, b, &fb) : j;
             for (int c = 0; c < cz; ++c) {
                 if (a == 0 && b == 0 && c == 0) {
                     continue;
                 }
+                int fc = -1;
+                const int kc = NDIM > 2 ? axis_target_at(k, p.nz, p.ng, p.bc.kind[4], p.bc.kind[5], sz, c, &fc) : k;
                 double qc[kMaxVars];
 #pragma unroll
                 for (int v = 0; v < kMaxVars; ++v) {
                     qc[v] = qn[v];
                 }
-                if (fx[a] >= 0) {
-                    bc_transform<NDIM>(p.bc, 0, fx[a], nvar, qc);
+                if (fa >= 0) {
+                    bc_transform<NDIM>(p.bc, 0, fa, nvar, qc);
                 }
-                if (fy[b] >= 0) {
-                    bc_transform<NDIM>(p.bc, 1, fy[b], nvar, qc);
+                if (fb >= 0) {
+                    bc_transform<NDIM>(p.bc, 1, fb, nvar, qc);
                 }
-                if (fz[c] >= 0) {
-                    bc_transform<NDIM>(p.bc, 2, fz[c], nvar, qc);
+                if (fc >= 0) {
+                    bc_transform<NDIM>(p.bc, 2, fc, nvar, qc);
                 }
+                double* dst = p.q_out + qidx(p, 0, kc, jb, ia);
 #pragma unroll
                 for (int v = 0; v < kMaxVars; ++v) {
                     if (v < nvar) {
-                        p.q_out[qidx(p, v, iz[c], iy[b], ix[a])] = qc[v];
+                        dst[v * vs] = qc[v];
                     }
                 }
                 account(qc);
@@ -491,7 +487,7 @@ __device__ __forceinline__ void segment1d(const StageParams& p, int x0, T* W, do
                 qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0);
             }
         }
-        dtmin = smin(write_cell<NDIM>(p, i, 0, 0, qn, p.last != 0, &flags), dtmin);
+        dtmin = smin(write_cell<NDIM, T>(p, i, 0, 0, qn, p.last != 0, &flags), dtmin);
     }
 }
 
@@ -716,7 +712,7 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
                         qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qt, 0.0);
                     }
                 }
-                dtmin = smin(write_cell<NDIM>(p, i, j, 0, qn, p.last != 0, &flags), dtmin);
+                dtmin = smin(write_cell<NDIM, T>(p, i, j, 0, qn, p.last != 0, &flags), dtmin);
             }
         }
         __syncthreads();
@@ -919,7 +915,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks2d) ztile3d_kernel(StagePa
                 qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qt, 0.0);
             }
         }
-        dtmin = smin(write_cell<NDIM>(p, i, j, kk, qn, p.last != 0, &flags), dtmin);
+        dtmin = smin(write_cell<NDIM, T>(p, i, j, kk, qn, p.last != 0, &flags), dtmin);
     }
     block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
 }
