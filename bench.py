@@ -153,16 +153,22 @@ def measured_peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic_per_launch():
-    """DRAM bytes per stage-kernel launch from the committed ncu summary."""
+def ncu_profile_value(key):
+    """A figure of the committed ncu summary of the headline stage kernel
+    (a line `key: value ...`)."""
     path = os.path.join(ROOT, "profiles", "stage2d_weno5z_hllc_kh2048_ncu.md")
     try:
         for ln in open(path):
-            if ln.startswith("traffic_bytes_per_launch:"):
+            if ln.startswith(key + ":"):
                 return float(ln.split(":")[1].split()[0])
     except OSError:
         pass
     return None
+
+
+def ncu_traffic_per_launch():
+    """DRAM bytes per stage-kernel launch from the committed ncu summary."""
+    return ncu_profile_value("traffic_bytes_per_launch")
 
 
 # ---------------------------------------------------------------------------
@@ -328,6 +334,13 @@ def run_ours(args):
                 "traffic": traffic, "peak_source": peak_kind, "kernel": kname,
                 "alg_bytes_per_launch": alg_bytes_per_launch, "avg_launch_ms": avg_launch_ms,
                 "launches_timed": stage_n}
+    if args.precision == "fp64":
+        # the bound the exact FP64 kernel actually meets: the FP64 pipe
+        # (IEEE divisions and square roots in the reference's order); its
+        # activity from the committed ncu capture of the same kernel
+        fp64_active = ncu_profile_value("fp64_pipe_active_frac")
+        roofline["compute"] = {"bound": "fp64 pipe", "active_frac_ncu": fp64_active,
+                               "source": "profiles/stage2d_weno5z_hllc_kh2048_ncu.md"}
 
     # the density after warmup + K steps, for the FP32 form's error
     rho64 = None

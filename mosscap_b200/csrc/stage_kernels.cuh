@@ -131,13 +131,29 @@ __device__ __forceinline__ double cfl_bound_of(const StageParams& p, const doubl
     }
 }
 
-// Write the new value of interior cell (i, j, k) and every ghost it is the
-// source of; returns the CFL minimum over the written values (last stage) and
+// Write the new value of interior cell (i, j, k); returns its CFL bound
+// (last stage) and ORs its status flags into *flags.
+template <int NDIM, class T = double>
+__device__ __forceinline__ double write_own(const StageParams& p, int i, int j, int k, const double* qn,
+                                            bool want_dt, unsigned* flags) {
+    const long long vs = (long long)p.zc * p.yc * p.xc;  // variable stride of the state
+    double* dst = p.q_out + qidx(p, 0, k, j, i);
+#pragma unroll
+    for (int v = 0; v < kMaxVars; ++v) {
+        if (v < p.nvar) {
+            dst[v * vs] = qn[v];
+        }
+    }
+    return want_dt ? cfl_bound_of<NDIM, T>(p, qn, flags) : __longlong_as_double(0x7ff0000000000000ll);
+}
+
+// Write every ghost that interior cell (i, j, k), of new value qn, is the
+// source of; returns the CFL minimum over the written ghosts (last stage) and
 // ORs their status flags into *flags. The ghost targets along each axis are
 // enumerated one at a time (axis_target_at), so nothing goes to local memory.
 template <int NDIM, class T = double>
-__device__ __forceinline__ double write_cell(const StageParams& p, int i, int j, int k, double* qn,
-                                             bool want_dt, unsigned* flags) {
+__device__ __forceinline__ double scatter_ghosts(const StageParams& p, int i, int j, int k, const double* qn,
+                                                 bool want_dt, unsigned* flags) {
     const int nvar = p.nvar;
     double dtmin = __longlong_as_double(0x7ff0000000000000ll);
     auto account = [&](const double* q) {
@@ -146,16 +162,6 @@ __device__ __forceinline__ double write_cell(const StageParams& p, int i, int j,
         }
     };
     const long long vs = (long long)p.zc * p.yc * p.xc;  // variable stride of the state
-    {
-        double* dst = p.q_out + qidx(p, 0, k, j, i);
-#pragma unroll
-        for (int v = 0; v < kMaxVars; ++v) {
-            if (v < nvar) {
-                dst[v * vs] = qn[v];
-            }
-        }
-    }
-    account(qn);
     const bool nx_ = near_face(i, p.nx, p.ng);
     const bool ny_ = NDIM > 1 && near_face(j, p.ny, p.ng);
     const bool nz_ = NDIM > 2 && near_face(k, p.nz, p.ng);
@@ -214,6 +220,16 @@ __device__ __forceinline__ double write_cell(const StageParams& p, int i, int j,
         }
     }
     return dtmin;
+}
+
+// Write the new value of interior cell (i, j, k) and every ghost it is the
+// source of; returns the CFL minimum over the written values (last stage) and
+// ORs their status flags into *flags.
+template <int NDIM, class T = double>
+__device__ __forceinline__ double write_cell(const StageParams& p, int i, int j, int k, double* qn,
+                                             bool want_dt, unsigned* flags) {
+    const double own = write_own<NDIM, T>(p, i, j, k, qn, want_dt, flags);
+    return smin(scatter_ghosts<NDIM, T>(p, i, j, k, qn, want_dt, flags), own);
 }
 
 // Primitives of a cell for the sweep of compute type T. T = double: the
@@ -915,7 +931,32 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks2d) ztile3d_kernel(StagePa
                 qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qt, 0.0);
             }
         }
-        dtmin = smin(write_cell<NDIM, T>(p, i, j, kk, qn, p.last != 0, &flags), dtmin);
+        dtmin = smin(write_own<NDIM, T>(p, i, j, kk, qn, p.last != 0, &flags), dtmin);
+    }
+    // the ghost scatter as a second loop, only in tiles with a cell next to
+    // a face: its registers stay out of the finishing loop above
+    const bool near_tile = (p.ng + x0 < 2 * p.ng) || (p.ng + x0 + vw - 1 >= p.nx) || near_face(j, p.ny, p.ng) ||
+                           (p.ng + z0 < 2 * p.ng) || (p.ng + z0 + vh - 1 >= p.nz);
+    if (near_tile) {
+#pragma unroll 1
+        for (int it = threadIdx.x; it < TZ * kZCols; it += kThreads) {
+            const int zr = it / kZCols;
+            const int x = it - zr * kZCols;
+            const int i = p.ng + x0 + x;
+            const int kk = p.ng + z0 + zr;
+            if (x >= vw || zr >= vh || !(near_face(i, p.nx, p.ng) || near_face(j, p.ny, p.ng) ||
+                                         near_face(kk, p.nz, p.ng))) {
+                continue;
+            }
+            // this thread's own store of the cell, read back
+            const long long id0 = qidx(p, 0, kk, j, i);
+            double qn[kMaxVars];
+#pragma unroll
+            for (int v = 0; v < kMaxVars; ++v) {
+                qn[v] = v < p.nvar ? p.q_out[id0 + v * vs] : 0.0;
+            }
+            dtmin = smin(scatter_ghosts<NDIM, T>(p, i, j, kk, qn, p.last != 0, &flags), dtmin);
+        }
     }
     block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
 }
