@@ -77,6 +77,32 @@ cudaError_t launch_tiled(const StageParams& p, const CUtensorMap& map, cudaStrea
     }
 }
 
+// The z pass with a TMA tile load where the staging area fits its CTAs per
+// SM, there are no tracers and the state's tensor map can be built.
+template <int REC>
+bool use_ztile_tma(const StageParams& p, CUtensorMap* map) {
+    if (!ztile_tma_capable<REC, Real>() || p.ntracer != 0) {
+        return false;
+    }
+    return tma_map_for(p.q_in, p.xc, p.yc, p.zc, p.nvar, kZStageX, 1, 5, map, ZTileGeom<REC>::WZ);
+}
+
+template <int REC, int LIM, int RS, bool TMA>
+cudaError_t launch_ztile(const StageParams& p, const CUtensorMap& map, cudaStream_t s) {
+    if constexpr (TMA && !ztile_tma_capable<REC, Real>()) {
+        return cudaErrorNotSupported;  // never taken: use_ztile_tma refused it
+    } else {
+        auto k = ztile3d_kernel<REC, LIM, RS, Real, MC_SRC, TMA>;
+        const size_t sm = TMA ? ztile_smem_bytes_tma<REC, Real>() : ztile_smem_bytes<REC, Real>(p.nvar);
+        cudaError_t e = allow_smem(k, sm);
+        if (e != cudaSuccess) {
+            return e;
+        }
+        k<<<dim3(cdiv(p.nz, kTile), cdiv(p.nx, kZCols), p.ny), dim3(kThreads), sm, s>>>(p, map);
+        return cudaGetLastError();
+    }
+}
+
 template <int REC, int LIM, int RS>
 cudaError_t launch_one(const StageParams& p, int pass, cudaStream_t s) {
 #if MC_DIM == 1
@@ -104,12 +130,10 @@ cudaError_t launch_one(const StageParams& p, int pass, cudaStream_t s) {
             return e;
         }
     } else {
-        auto k = ztile3d_kernel<REC, LIM, RS, Real, MC_SRC>;
-        const size_t sm = ztile_smem_bytes<REC, Real>(p.nvar);
-        cudaError_t e = allow_smem(k, sm);
-        if (e == cudaSuccess) {
-            k<<<dim3(cdiv(p.nz, kTile), cdiv(p.nx, kZCols), p.ny), dim3(kThreads), sm, s>>>(p);
-        }
+        CUtensorMap map;
+        std::memset(&map, 0, sizeof(map));
+        const cudaError_t e = use_ztile_tma<REC>(p, &map) ? launch_ztile<REC, LIM, RS, true>(p, map, s)
+                                                          : launch_ztile<REC, LIM, RS, false>(p, map, s);
         if (e != cudaSuccess) {
             return e;
         }

@@ -810,6 +810,27 @@ __host__ __device__ constexpr size_t ztile_smem_bytes(int nvar) {
     return sizeof(T) * (size_t)nvar * ZTileGeom<REC>::WV;
 }
 
+// The z pass with a TMA tile load: the conserved tile (kZStageX x-columns
+// from the even column at or before the tile's first, one y row, WZ z rows,
+// five variables, doubles) is staged by one tensor copy ahead of the
+// primitive tile W; it stays there for the finishing phase, which takes each
+// cell's stage input from it. 128 bytes of slack align the staging area.
+constexpr int kZStageX = kZCols + 2;
+template <int REC>
+__host__ __device__ constexpr size_t ztile_stage_bytes() {
+    return sizeof(double) * 5 * (size_t)ZTileGeom<REC>::WZ * kZStageX;
+}
+template <int REC, class T>
+__host__ __device__ constexpr size_t ztile_smem_bytes_tma() {
+    return 128 + ztile_stage_bytes<REC>() + ztile_smem_bytes<REC, T>(5);
+}
+// CTAs per SM of the z pass: three (80 registers); the TMA form only where
+// its staging area still lets three fit (the FP32 form: 72.8 KB per CTA).
+template <int REC, class T>
+__host__ __device__ constexpr bool ztile_tma_capable() {
+    return (size_t)kMinBlocks2d * (ztile_smem_bytes_tma<REC, T>() + 1024 + 256) <= 233472;
+}
+
 // z pass: each CTA loads the primitives of its tile, sweeps every column
 // along z with one warp (lane L reconstructs cell L-1 of the column, solves
 // the face below it, and takes the next face's flux from lane L+1, exactly
@@ -821,8 +842,14 @@ __host__ __device__ constexpr size_t ztile_smem_bytes(int nvar) {
 // fastest, so the halo rows a neighbouring chunk re-reads are still in L2.
 // Three CTAs per SM in both precisions: at four (64 registers) the FP32 z
 // pass spilled 196 bytes per thread.
-template <int REC, int LIM, int RS, class T, bool SRC = false>
-__global__ void __launch_bounds__(kThreads, kMinBlocks2d) ztile3d_kernel(StageParams p) {
+//
+// TMA (no tracers, even row length; see ztile_tma_capable): the conserved
+// tile arrives by one tensor copy (tmap: 4D x, y, z, var; box kZStageX x 1 x
+// WZ x 5) completed on an mbarrier with a bounded wait, and the finishing
+// phase reads each cell's stage input from it.
+template <int REC, int LIM, int RS, class T, bool SRC = false, bool TMA = false>
+__global__ void __launch_bounds__(kThreads, kMinBlocks2d)
+    ztile3d_kernel(StageParams p, const __grid_constant__ CUtensorMap tmap) {
     if (p.dt_dev && p.blk->done) {
         return;
     }
@@ -834,7 +861,16 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks2d) ztile3d_kernel(StagePa
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red_d[kWarps];
     __shared__ unsigned red_u[kWarps];
-    T* W = reinterpret_cast<T*>(smem_raw);
+    __shared__ __align__(8) uint64_t mbar;
+    T* W;
+    double* stg = nullptr;
+    if constexpr (TMA) {
+        unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+        stg = reinterpret_cast<double*>(base);
+        W = reinterpret_cast<T*>(base + ztile_stage_bytes<REC>());
+    } else {
+        W = reinterpret_cast<T*>(smem_raw);
+    }
 
     const int z0 = blockIdx.x * TZ;
     const int x0 = blockIdx.y * kZCols;
@@ -846,13 +882,45 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks2d) ztile3d_kernel(StagePa
     double dtmin = __longlong_as_double(0x7ff0000000000000ll);
 
     // phase 1: primitives of the tile and its halo rows
-    for (int it = threadIdx.x; it < WZ * kZCols; it += kThreads) {
-        const int r = it / kZCols;
-        const int x = it - r * kZCols;
-        const int i = p.ng + x0 + x;
-        const int k = p.ng + z0 - H + r;
-        const bool inb = x < vw && k >= 0 && k < p.zc;
-        flags |= load_prim<NDIM, T>(p, k, j, i, inb, W + r * PZ + x, WV);
+    // (TMA: column x of the tile is column x + xoff of the staged box)
+    const int xoff = (p.ng + x0) & 1;
+    if constexpr (TMA) {
+        if (threadIdx.x == 0) {
+            mbar_init(&mbar, 1);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            mbar_expect_tx(&mbar, (uint32_t)ztile_stage_bytes<REC>());
+            tma_load_4d(stg, &tmap, p.ng + x0 - xoff, j, p.ng + z0 - H, 0, &mbar);
+        }
+        const bool ok = mbar_wait_bounded(&mbar, 0, kTmaWaitPolls);
+        if (!__syncthreads_and(ok)) {
+            // the copy did not complete: raise the flag, give the copy in
+            // flight one more bounded wait, and leave the tile unwritten
+            if (threadIdx.x == 0) {
+                atomicOr(&p.blk->status, 0x20u);
+            }
+            mbar_wait_bounded(&mbar, 0, kTmaWaitPolls);
+            __syncthreads();
+            return;
+        }
+        constexpr int SV = WZ * kZStageX;  // per-variable stride of the staged box
+        for (int it = threadIdx.x; it < WZ * kZCols; it += kThreads) {
+            const int r = it / kZCols;
+            const int x = it - r * kZCols;
+            const int k = p.ng + z0 - H + r;
+            const bool inb = x < vw && k >= 0 && k < p.zc;
+            flags |= staged_prim<NDIM, T>(p, stg + r * kZStageX + x + xoff, SV, inb, W + r * PZ + x, WV);
+        }
+    } else {
+        for (int it = threadIdx.x; it < WZ * kZCols; it += kThreads) {
+            const int r = it / kZCols;
+            const int x = it - r * kZCols;
+            const int i = p.ng + x0 + x;
+            const int k = p.ng + z0 - H + r;
+            const bool inb = x < vw && k >= 0 && k < p.zc;
+            flags |= load_prim<NDIM, T>(p, k, j, i, inb, W + r * PZ + x, WV);
+        }
     }
     __syncthreads();
 
@@ -905,7 +973,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks2d) ztile3d_kernel(StagePa
 #pragma unroll
         for (int v = 0; v < nh; ++v) {
             qu[v] = p.dqxy[v * cells + o];
-            qi[v] = p.q_in[id0 + v * vs];
+            if constexpr (TMA) {
+                qi[v] = stg[(v * WZ + zr + H) * kZStageX + x + xoff];
+            } else {
+                qi[v] = p.q_in[id0 + v * vs];
+            }
             qo[v] = old ? p.q_old[id0 + v * vs] : 0.0;
         }
         source_dt_of<NDIM, SRC>(p, qi, dt, sdt);

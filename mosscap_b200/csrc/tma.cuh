@@ -83,11 +83,12 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
 constexpr int kTmaWaitPolls = 1 << 20;
 
 // Host: the tensor map of state array q ([nvar][zc][yc][xc] doubles) whose
-// box is box_x x box_y cells (x, y), one plane, nv variables; the tensor is
+// box is box_x x box_y x box_z cells (x, y, z), nv variables; the tensor is
 // 3D (x, y, var) when zc == 1, else 4D (x, y, z, var). Returns false (and
 // the caller falls back to per-thread loads) when the array cannot be
 // described: base not 16-byte aligned, a row pitch that is not a multiple of
-// 16 bytes, or the driver refuses the map.
-bool tma_map_for(const double* q, int xc, int yc, int zc, int nvar, int box_x, int box_y, int nv, CUtensorMap* out);
+// 16 bytes, a box larger than the array, or the driver refuses the map.
+bool tma_map_for(const double* q, int xc, int yc, int zc, int nvar, int box_x, int box_y, int nv, CUtensorMap* out,
+                 int box_z = 1);
 
 } // namespace mc
