@@ -34,6 +34,12 @@ template <class T>
 __device__ __forceinline__ T sq(T a) {
     return a * a;
 }
+// a * b + c. For T = double in the exact translation units (compiled without
+// contraction) this is the product and then the sum, as written.
+template <class T>
+__device__ __forceinline__ T madd(T a, T b, T c) {
+    return a * b + c;
+}
 
 // Half-width of the reconstruction stencil: cells c-S..c+S are read to
 // reconstruct the faces of cell c (source/Reconstruct.hpp:95-123, :150-274).
@@ -225,36 +231,40 @@ __device__ __forceinline__ void reconstruct(const T* s, T& wl, T& wr) {
         wr = r;
     } else {
         // WENO5-Z (Borges et al. 2008) with the Z+ style indicator tau5 /
-        // (beta_k + eps) squared; candidate stencils pre-multiplied by 6 (:217-274)
-        const T b_a = T(13) / T(12);
+        // (beta_k + eps) squared; candidate stencils pre-multiplied by 6 (:217-274).
+        // The reference's expression trees; madd(a, b, c) is a * b + c and
+        // only commutes an addition's operands where it appears, so the
+        // exact FP64 results are unchanged. 13 / 12 is the same correctly
+        // rounded constant as the reference's T(13) / T(12).
+        const T b_a = T(13.0 / 12.0);
         const T b_b = T(0.25);
-        const T beta0 = b_a * sq(s[0] - T(2) * s[1] + c) + b_b * sq(s[0] - T(4) * s[1] + T(3) * c);
-        const T beta1 = b_a * sq(s[1] - T(2) * c + s[3]) + b_b * sq(s[1] - s[3]);
-        const T beta2 = b_a * sq(c - T(2) * s[3] + s[4]) + b_b * sq(T(3) * c - T(4) * s[3] + s[4]);
+        const T beta0 = madd(b_a, sq(s[0] - T(2) * s[1] + c), b_b * sq(s[0] - T(4) * s[1] + T(3) * c));
+        const T beta1 = madd(b_a, sq(s[1] - T(2) * c + s[3]), b_b * sq(s[1] - s[3]));
+        const T beta2 = madd(b_a, sq(c - T(2) * s[3] + s[4]), b_b * sq(T(3) * c - T(4) * s[3] + s[4]));
         const T eps = Consts<T>::weno_eps;
         const T tau5 = fabs(beta0 - beta2);
         const T ind0 = tau5 / (beta0 + eps);
         const T ind1 = tau5 / (beta1 + eps);
         const T ind2 = tau5 / (beta2 + eps);
         {
-            const T e0 = (T(2) * c + T(5) * s[1] - s[0]);
-            const T e1 = (-s[3] + T(5) * c + T(2) * s[1]);
-            const T e2 = (T(2) * s[4] - T(7) * s[3] + T(11) * c);
-            const T a0 = T(3) * (T(1) + sq(ind0));
-            const T a1 = T(6) * (T(1) + sq(ind1));
-            const T a2 = T(1) + sq(ind2);
+            const T e0 = (madd(T(2), c, T(5) * s[1]) - s[0]);
+            const T e1 = (madd(T(2), s[1], -s[3] + T(5) * c));
+            const T e2 = (madd(T(11), c, T(2) * s[4] - T(7) * s[3]));
+            const T a0 = T(3) * madd(ind0, ind0, T(1));
+            const T a1 = T(6) * madd(ind1, ind1, T(1));
+            const T a2 = madd(ind2, ind2, T(1));
             const T den = T(6) * (a0 + a1 + a2);
-            wl = (e0 * a0 + e1 * a1 + e2 * a2) / den;
+            wl = madd(e2, a2, madd(e1, a1, e0 * a0)) / den;
         }
         {
-            const T e0 = (T(2) * c + T(5) * s[3] - s[4]);
-            const T e1 = (-s[1] + T(5) * c + T(2) * s[3]);
-            const T e2 = (T(2) * s[0] - T(7) * s[1] + T(11) * c);
-            const T a0 = T(3) * (T(1) + sq(ind2));
-            const T a1 = T(6) * (T(1) + sq(ind1));
-            const T a2 = T(1) + sq(ind0);
+            const T e0 = (madd(T(2), c, T(5) * s[3]) - s[4]);
+            const T e1 = (madd(T(2), s[3], -s[1] + T(5) * c));
+            const T e2 = (madd(T(11), c, T(2) * s[0] - T(7) * s[1]));
+            const T a0 = T(3) * madd(ind2, ind2, T(1));
+            const T a1 = T(6) * madd(ind1, ind1, T(1));
+            const T a2 = madd(ind0, ind0, T(1));
             const T den = T(6) * (a0 + a1 + a2);
-            wr = (e0 * a0 + e1 * a1 + e2 * a2) / den;
+            wr = madd(e2, a2, madd(e1, a1, e0 * a0)) / den;
         }
     }
 }
