@@ -358,6 +358,51 @@ mc_status mc_adjoint_forward(mc_adjoint* adj, double* Q, const mc_clock* clock, 
  * stream when dgamma is not NULL. */
 mc_status mc_adjoint_backward(mc_adjoint* adj, double* lambda, double* dgamma, void* stream);
 
+/* Slab decomposition of the adjoint over ranks (one GPU per rank). The
+ * periodic 2D problem is split along y into one slab per rank, ranks in y
+ * order (rank 0 the lowest rows, at least 5 rows each); each rank creates
+ * its mc_adjoint for its own slab (grid = its rows with ghost layers) and
+ * joins before mc_adjoint_forward, with the id of mc_slab_unique_id
+ * (collective, as mc_set_slab_decomposition). Then:
+ *   forward: the ghost rows between slabs are exchanged after every stage
+ *     (and once on entry, so the caller's y ghosts are not read) and every dt
+ *     is the all-reduce MIN of the ranks' CFL minima: the slabs together
+ *     advance bit-identically to the single domain;
+ *   backward: the reverse sweep is the transpose of that exchange. The
+ *     cotangent of a cell comes from the faces whose stencils read it,
+ *     including the faces just across a slab border, which a neighbour's
+ *     cells own: before every stage's product each rank receives the 5
+ *     bordering rows of the stage input and the 3 bordering rows of the
+ *     stage cotangent from each neighbour and recomputes those faces'
+ *     contributions to its own cells itself (a gather rather than a
+ *     scatter-and-add of ghost cotangents, so no cell is written by two
+ *     ranks). Each step's dt sensitivity is summed over the ranks and routed
+ *     to the lowest-index global CFL arg-min cell, on the rank that owns it;
+ *     dJ/dgamma is summed over the ranks at the end.
+ * Per-cell arithmetic is that of the single domain; the sums of the dt and
+ * gamma sensitivities change order with the partition (rounding-level
+ * differences with world > 1; bit-identical with world = 1). */
+mc_status mc_adjoint_set_slab_decomposition(mc_adjoint* adj, const uint8_t* id, int32_t rank, int32_t world);
+
+/* The same decomposition with the caller moving the data: the library calls
+ * fn(user, op, bufs, count, stream) wherever it would call NCCL, with device
+ * buffers and work enqueued on `stream` before it; fn returns 0 on success,
+ * any other value fails the library call with MC_ERR_CUDA. Every rank makes
+ * the same calls in the same order.
+ *   MC_COMM_HALO: bufs = {send_lo, send_hi, recv_lo, recv_hi}, count
+ *     doubles each: send_lo to the rank below (rank-1, periodic), which
+ *     receives it in its recv_hi; send_hi to the rank above, into its recv_lo.
+ *   MC_COMM_MIN_U64 / MC_COMM_SUM_F64 / MC_COMM_MIN_I64: bufs[0], count
+ *     elements, all-reduced in place. */
+typedef enum {
+    MC_COMM_HALO = 0,
+    MC_COMM_MIN_U64 = 1,
+    MC_COMM_SUM_F64 = 2,
+    MC_COMM_MIN_I64 = 3
+} mc_comm_op;
+typedef int32_t (*mc_comm_fn)(void* user, int32_t op, void* const* bufs, int64_t count, void* stream);
+mc_status mc_adjoint_set_slab_hook(mc_adjoint* adj, mc_comm_fn fn, void* user, int32_t rank, int32_t world);
+
 /* Tangent-linear (forward-mode) derivative of n_steps steps of the scheme the
  * adjoint covers (2D, WENO5-Z + HLLC, FP64, periodic faces, any stepper),
  * with dt = compute_dt under *clock each step: Q (device, ghosts filled or

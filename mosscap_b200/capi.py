@@ -77,6 +77,10 @@ class McBatchProblem(ctypes.Structure):
 USER_BC_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
 # void (*)(void* user, uint64_t* cfl_min_bits, void* stream)
 CFL_REDUCE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
+# int32_t (*)(void* user, int32_t op, void* const* bufs, int64_t count, void* stream)
+COMM_FN = ctypes.CFUNCTYPE(ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p),
+                           ctypes.c_int64, ctypes.c_void_p)
+COMM_HALO, COMM_MIN_U64, COMM_SUM_F64, COMM_MIN_I64 = 0, 1, 2, 3
 
 
 class McEosTable(ctypes.Structure):
@@ -177,6 +181,10 @@ def load() -> ctypes.CDLL:
     lib.mc_adjoint_forward.restype = i32
     lib.mc_adjoint_backward.argtypes = [vp, vp, P(d), vp]
     lib.mc_adjoint_backward.restype = i32
+    lib.mc_adjoint_set_slab_decomposition.argtypes = [vp, ctypes.c_char_p, i32, i32]
+    lib.mc_adjoint_set_slab_decomposition.restype = i32
+    lib.mc_adjoint_set_slab_hook.argtypes = [vp, COMM_FN, vp, i32, i32]
+    lib.mc_adjoint_set_slab_hook.restype = i32
     lib.mc_debug_reverse_reciprocal.argtypes = [vp, vp, i64, vp]
     lib.mc_debug_reverse_reciprocal.restype = i32
     if lib.mc_abi_version() != 1:

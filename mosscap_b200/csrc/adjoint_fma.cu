@@ -16,6 +16,10 @@
 //           g_gamma += b dt <lam_out, dL/dgamma>
 // and each step's g_dt flows back through dt = max_cfl * dx / (c_s + |v|)
 // at the arg-min cell (unless the step's dt was clamped to an output time).
+// Split into y slabs over ranks (mc_adjoint_set_slab_*), the forward and the
+// recompute exchange ghost rows after every stage, and each stage's product
+// reads the bordering rows of its input and cotangent from the neighbours
+// (halo buffers) instead of wrapping around the slab.
 // The reverse sweep's own arithmetic need not be bit-exact, so this unit is
 // compiled with multiply-add contraction; the forward recompute (the stage
 // kernels), the arg-min search and the recording clock run in units compiled
@@ -31,6 +35,7 @@
 #include "adjoint_physics.cuh"
 #include "launch.h"
 #include "mosscap_b200.h"
+#include "slab.h"
 
 using mc::DeviceBlock;
 using mc::StageParams;
@@ -67,6 +72,13 @@ struct VjpParams {
     const double* acc_in;   // optional accumulator of the step-start cotangent
     double* acc_out;        // optional: acc_out = acc_in + a * mu
     const double* dt;       // device dt of the step
+    // Rows beyond the slab (slab decomposition; NULL: periodic wrap within
+    // the grid): [4][kAH][xc] rows -kAH .. -1 and ny .. ny + kAH - 1 of the
+    // stage input, [4][kMH][xc] the same of the cotangent.
+    const double* qlo;
+    const double* qhi;
+    const double* mlo;
+    const double* mhi;
     double a, b;
     double dx, gamma;
     int nx, ny, ng, xc, yc;
@@ -81,6 +93,24 @@ __device__ __forceinline__ int wrap(int i, int n) {
 
 __device__ __forceinline__ long long pidx(const VjpParams& p, int v, int j, int i) {
     return ((long long)v * p.yc + j) * (long long)p.xc + i;
+}
+
+// Variable v of the cell in padded column i and slab row gy (gy >= -H): own
+// rows from the state, rows beyond the slab from the H-row halo of the
+// neighbour (rows past the halo, which no own cell's result reads, repeat
+// its last row), or without halos the periodic image.
+__device__ __forceinline__ double slab_at(const VjpParams& p, const double* own, const double* lo, const double* hi,
+                                          int H, int v, int gy, int i) {
+    if (!lo) {
+        return own[pidx(p, v, p.ng + wrap(gy, p.ny), i)];
+    }
+    if (gy < 0) {
+        return lo[((long long)v * H + gy + H) * p.xc + i];
+    }
+    if (gy >= p.ny) {
+        return hi[((long long)v * H + min(gy - p.ny, H - 1)) * p.xc + i];
+    }
+    return own[pidx(p, v, p.ng + gy, i)];
 }
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
@@ -132,11 +162,11 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
                 tx = r - hr * AT;
                 ty = hr < kAH ? hr - kAH : AT + hr - kAH;
             }
-            const int i = p.ng + wrap(x0 + tx, p.nx), j = p.ng + wrap(y0 + ty, p.ny);
+            const int i = p.ng + wrap(x0 + tx, p.nx);
             double q[4], w[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
-                q[v] = p.q[pidx(p, v, j, i)];
+                q[v] = slab_at(p, p.q, p.qlo, p.qhi, kAH, v, y0 + ty, i);
             }
             mc::prim_from_cons_rev2(K.gm1, q, w);
 #pragma unroll
@@ -157,10 +187,10 @@ __global__ void __launch_bounds__(kAThreads, 2) stage_vjp_kernel(VjpParams p) {
                 tx = r - hr * AT;
                 ty = hr < kMH ? hr - kMH : AT + hr - kMH;
             }
-            const int i = p.ng + wrap(x0 + tx, p.nx), j = p.ng + wrap(y0 + ty, p.ny);
+            const int i = p.ng + wrap(x0 + tx, p.nx);
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
-                MU[(v * kMW + ty + kMH) * kMP + tx + kMH] = p.mu[pidx(p, v, j, i)];
+                MU[(v * kMW + ty + kMH) * kMP + tx + kMH] = slab_at(p, p.mu, p.mlo, p.mhi, kMH, v, y0 + ty, i);
             }
         }
         for (int it = threadIdx.x; it < 4 * AT * kBP; it += kAThreads) {
@@ -311,17 +341,25 @@ __global__ void reduce_stage_kernel(const double* part_gdt, const double* part_g
     }
 }
 
+// The arg-min cell as a key ordered like global cell indices over y slabs:
+// (rank << 32) | local index, or the largest key when this rank holds none.
+__global__ void argmin_key_kernel(const int* idx, int rank, long long* key) {
+    *key = *idx == 0x7fffffff ? 0x7fffffffffffffffLL : ((long long)rank << 32) | (long long)*idx;
+}
+
 // Close one step of the reverse sweep: route the step's dt sensitivity to
-// the arg-min cell (unless the output clamp fixed dt), then clear it.
+// the arg-min cell (unless the output clamp fixed dt) on the rank that owns
+// it, then clear it.
 __global__ void dt_vjp_kernel(const double* q, int nx, int ng, int xc, int yc, double gamma, double dx,
-                              double max_cfl, const int* idx, const int* clamped, double* step_gdt, double* lam,
-                              double* gamma_bar) {
+                              double max_cfl, const long long* key, int rank, const int* clamped, double* step_gdt,
+                              double* lam, double* gamma_bar) {
     const double g = *step_gdt;
     *step_gdt = 0.0;
-    if (*clamped || *idx == 0x7fffffff || g == 0.0) {
+    const long long k_ = *key;
+    if (*clamped || k_ == 0x7fffffffffffffffLL || (int)(k_ >> 32) != rank || g == 0.0) {
         return;
     }
-    const int c = *idx;
+    const int c = (int)(k_ & 0xffffffffLL);
     const int xi = c % nx, yi = c / nx;
     const long long plane = (long long)xc * yc;
     const long long cell = (long long)(yi + ng) * xc + xi + ng;
@@ -343,6 +381,21 @@ __global__ void dt_vjp_kernel(const double* q, int nx, int ng, int xc, int yc, d
 __global__ void reciprocal_kernel(const double* x, double* out, long long n) {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
         out[k] = mc::arcp(x[k]);
+    }
+}
+
+// Rows of the 4 variables between the padded state and contiguous
+// [4][rows][xc] blocks, two blocks per launch: dst_b[v * dst_stride + k] =
+// src_b[v * src_stride + k] for k < len, b = 0, 1.
+__global__ void copy_rows_kernel(const double* src0, const double* src1, double* dst0, double* dst1,
+                                 long long src_stride, long long dst_stride, long long len) {
+    const long long n = 8 * len;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(t / (4 * len));
+        const long long r = t - b * 4 * len;
+        const int v = (int)(r / len);
+        const long long k = r - v * len;
+        (b ? dst1 : dst0)[v * dst_stride + k] = (b ? src1 : src0)[v * src_stride + k];
     }
 }
 
@@ -379,8 +432,18 @@ struct mc_adjoint {
     double* part = nullptr;     // 2 x tiles partial sums
     double* scal = nullptr;     // [0] step g_dt, [1] gamma bar
     int* argmin = nullptr;
+    long long* key = nullptr;   // arg-min key (argmin_key_kernel)
     int tiles = 0;
     bool recorded = false;
+    // slab decomposition along y (mc_adjoint_set_slab_*)
+    bool sliced = false;
+    int rank = 0, world = 1;
+    mc::SlabExchange* slab = nullptr;  // NCCL, or
+    mc_comm_fn comm_fn = nullptr;      // the caller's hook
+    void* comm_user = nullptr;
+    long long halo_cap = 0;            // doubles per send / receive block: 4 (kAH + kMH) xc
+    double* send = nullptr;            // [2][halo_cap]: to the rank below, to the rank above
+    double* recv = nullptr;            // [2][halo_cap]: from the rank below, from the rank above
 };
 
 namespace {
@@ -416,12 +479,101 @@ StageParams fwd_params(const mc_adjoint* a) {
     for (int f = 0; f < 6; ++f) {
         p.bc.kind[f] = f < 4 ? MC_BC_PERIODIC : MC_BC_USERFN;
     }
+    if (a->sliced) {
+        // the exchange fills the ghost rows between slabs
+        p.bc.kind[2] = p.bc.kind[3] = MC_BC_USERFN;
+    }
     return p;
 }
 
-// One SSPRK3 stage of the forward scheme (the fused FP64 kernel). The
-// recompute of the reverse sweep runs on its own control block, which never
-// marks the loop done.
+mc_status comm_halo(mc_adjoint* a, long long count, cudaStream_t s) {
+    double* slo = a->send;
+    double* shi = a->send + a->halo_cap;
+    double* rlo = a->recv;
+    double* rhi = a->recv + a->halo_cap;
+    if (a->slab) {
+        const char* why = "";
+        if (mc::slab_halo(a->slab, slo, shi, rlo, rhi, (size_t)count, s, &why) != cudaSuccess) {
+            return afail(MC_ERR_CUDA, std::string("slab halo exchange: ") + why);
+        }
+        return MC_OK;
+    }
+    void* bufs[4] = {slo, shi, rlo, rhi};
+    if (a->comm_fn(a->comm_user, MC_COMM_HALO, bufs, count, (void*)s) != 0) {
+        return afail(MC_ERR_CUDA, "slab hook: halo exchange failed");
+    }
+    return MC_OK;
+}
+
+mc_status comm_reduce(mc_adjoint* a, mc_comm_op op, void* buf, cudaStream_t s) {
+    if (a->slab) {
+        const mc::SlabReduce r = op == MC_COMM_MIN_U64   ? mc::SlabReduce::kMinU64
+                                 : op == MC_COMM_SUM_F64 ? mc::SlabReduce::kSumF64
+                                                         : mc::SlabReduce::kMinI64;
+        const char* why = "";
+        if (mc::slab_all_reduce(a->slab, buf, 1, r, s, &why) != cudaSuccess) {
+            return afail(MC_ERR_CUDA, std::string("slab all-reduce: ") + why);
+        }
+        return MC_OK;
+    }
+    void* bufs[4] = {buf, nullptr, nullptr, nullptr};
+    if (a->comm_fn(a->comm_user, op, bufs, 1, (void*)s) != 0) {
+        return afail(MC_ERR_CUDA, "slab hook: all-reduce failed");
+    }
+    return MC_OK;
+}
+
+int copy_blocks(long long len) {
+    const long long b = (8 * len + 255) / 256;
+    return (int)(b < 148 * 4 ? b : 148 * 4);
+}
+
+// Ghost rows between slabs: this slab's first / last ng rows to the ranks
+// below / above, their bordering rows into its ghost rows.
+mc_status exchange_ghosts(mc_adjoint* a, double* q, cudaStream_t s) {
+    if (!a->sliced) {
+        return MC_OK;
+    }
+    const long long xc = a->grid.xc, ng = a->grid.ng, ny = a->ny;
+    const long long len = ng * xc;
+    copy_rows_kernel<<<copy_blocks(len), 256, 0, s>>>(q + ng * xc, q + ny * xc, a->send, a->send + a->halo_cap,
+                                                      a->plane, len, len);
+    MCA_CUDA(cudaGetLastError(), "pack ghost rows");
+    if (mc_status st = comm_halo(a, 4 * len, s)) {
+        return st;
+    }
+    copy_rows_kernel<<<copy_blocks(len), 256, 0, s>>>(a->recv, a->recv + a->halo_cap, q, q + (ny + ng) * xc, len,
+                                                      a->plane, len);
+    MCA_CUDA(cudaGetLastError(), "unpack ghost rows");
+    return MC_OK;
+}
+
+// The rows a stage's product reads beyond the slab: kAH rows of the stage
+// input and kMH rows of its cotangent from each neighbour, into the receive
+// blocks ([4][kAH][xc] then [4][kMH][xc] in each).
+mc_status exchange_vjp_halo(mc_adjoint* a, const double* q, const double* mu, cudaStream_t s) {
+    const long long xc = a->grid.xc, ng = a->grid.ng, ny = a->ny;
+    const long long lq = kAH * xc, lm = kMH * xc;
+    copy_rows_kernel<<<copy_blocks(lq), 256, 0, s>>>(q + ng * xc, q + (ng + ny - kAH) * xc, a->send,
+                                                     a->send + a->halo_cap, a->plane, lq, lq);
+    MCA_CUDA(cudaGetLastError(), "pack halo rows");
+    copy_rows_kernel<<<copy_blocks(lm), 256, 0, s>>>(mu + ng * xc, mu + (ng + ny - kMH) * xc, a->send + 4 * lq,
+                                                     a->send + a->halo_cap + 4 * lq, a->plane, lm, lm);
+    MCA_CUDA(cudaGetLastError(), "pack cotangent halo rows");
+    return comm_halo(a, a->halo_cap, s);
+}
+
+// The CFL minimum word of the forward's control block, reduced over the slabs.
+mc_status reduce_cfl_word(mc_adjoint* a, cudaStream_t s) {
+    if (!a->sliced) {
+        return MC_OK;
+    }
+    return comm_reduce(a, MC_COMM_MIN_U64, &a->blk->cfl_min_bits, s);
+}
+
+// One SSPRK3 stage of the forward scheme (the fused FP64 kernel), then the
+// ghost rows between slabs. The recompute of the reverse sweep runs on its
+// own control block, which never marks the loop done.
 mc_status fwd_stage(mc_adjoint* a, const double* in, const double* old_, double* out, int combo, int last,
                     const double* dt_dev, cudaStream_t s, bool recompute = false) {
     StageParams p = fwd_params(a);
@@ -436,7 +588,7 @@ mc_status fwd_stage(mc_adjoint* a, const double* in, const double* old_, double*
     p.last = last;
     MCA_CUDA(mc::launch_stage_d2_fp64(p, MC_RECON_WENO5Z, MC_LIMITER_MONOTONIZED_CENTRAL, MC_RIEMANN_HLLC, 0, s),
              "forward stage");
-    return MC_OK;
+    return exchange_ghosts(a, out, s);
 }
 
 mc_status grow(mc_adjoint* a, int64_t steps) {
@@ -449,7 +601,8 @@ mc_status grow(mc_adjoint* a, int64_t steps) {
         MCA_CUDA(cudaMalloc(&a->seg, sizeof(double) * a->state * (3 * (size_t)k_eff + 1)), "alloc segment");
         a->seg_cap = k_eff;
     }
-    if (steps <= a->rec_cap) {
+    // the records hold steps + 1 entries (a run of 0 steps still records its first dt)
+    if (a->dts && a->mins && a->clamped && a->ckpt && steps <= a->rec_cap) {
         return MC_OK;
     }
     cudaFree(a->dts);
@@ -479,6 +632,15 @@ mc_status vjp_stage(mc_adjoint* a, const double* q, const double* mu, double* la
     p.acc_in = acc_in;
     p.acc_out = acc_out;
     p.dt = dt;
+    if (a->sliced) {
+        if (mc_status st = exchange_vjp_halo(a, q, mu, s)) {
+            return st;
+        }
+        p.qlo = a->recv;
+        p.mlo = a->recv + 4 * kAH * (long long)a->grid.xc;
+        p.qhi = a->recv + a->halo_cap;
+        p.mhi = p.qhi + 4 * kAH * (long long)a->grid.xc;
+    }
     p.a = coef_a;
     p.b = coef_b;
     p.dx = a->grid.dx;
@@ -496,6 +658,31 @@ mc_status vjp_stage(mc_adjoint* a, const double* q, const double* mu, double* la
     reduce_stage_kernel<<<1, 256, 0, s>>>(a->part, a->part + a->tiles, a->tiles, coef_b / a->grid.dx, a->scal,
                                           a->scal + 1);
     MCA_CUDA(cudaGetLastError(), "reduce");
+    return MC_OK;
+}
+
+// Checks and buffers shared by both forms of the slab decomposition.
+mc_status slab_prepare(mc_adjoint* a, int32_t rank, int32_t world) {
+    if (!a || world < 1 || rank < 0 || rank >= world) {
+        return afail(MC_ERR_INVALID_ARGUMENT, "null adjoint or rank outside [0, world)");
+    }
+    if (a->sliced) {
+        return afail(MC_ERR_INVALID_ARGUMENT, "the adjoint already holds a slab decomposition");
+    }
+    if (a->recorded) {
+        return afail(MC_ERR_INVALID_ARGUMENT, "join the slab decomposition before the forward run");
+    }
+    if (a->ny < kAH || a->ny < a->grid.ng) {
+        return afail(MC_ERR_INVALID_ARGUMENT, "a slab needs at least max(5, ng) rows");
+    }
+    // one block holds the VJP halos ([4][kAH][xc] + [4][kMH][xc]) or ng ghost rows
+    a->halo_cap = 4LL * (kAH + kMH > a->grid.ng ? kAH + kMH : a->grid.ng) * a->grid.xc;
+    if (!a->send) {
+        MCA_CUDA(cudaMalloc(&a->send, sizeof(double) * 2 * (size_t)a->halo_cap), "alloc halo");
+    }
+    if (!a->recv) {
+        MCA_CUDA(cudaMalloc(&a->recv, sizeof(double) * 2 * (size_t)a->halo_cap), "alloc halo");
+    }
     return MC_OK;
 }
 
@@ -557,6 +744,7 @@ mc_status mc_adjoint_create(const mc_grid* grid, const mc_scheme* scheme, int32_
     alloc((void**)&a->part, sizeof(double) * 2 * a->tiles);
     alloc((void**)&a->scal, sizeof(double) * 2);
     alloc((void**)&a->argmin, sizeof(int));
+    alloc((void**)&a->key, sizeof(long long));
     if (e == cudaSuccess) {
         e = cudaFuncSetAttribute(stage_vjp_kernel<kTile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)VjpTile<kTile>::smem_bytes());
@@ -589,6 +777,10 @@ mc_status mc_adjoint_destroy(mc_adjoint* a) {
     cudaFree(a->part);
     cudaFree(a->scal);
     cudaFree(a->argmin);
+    cudaFree(a->key);
+    cudaFree(a->send);
+    cudaFree(a->recv);
+    mc::slab_destroy(a->slab);
     delete a;
     return MC_OK;
 }
@@ -605,9 +797,15 @@ mc_status mc_adjoint_forward(mc_adjoint* a, double* Q, const mc_clock* clock, in
     MCA_CUDA(mc::launch_clock_init(a->blk, clock->time, clock->max_time, clock->prev_output_time,
                                    clock->output_delta, a->scheme.max_cfl, s),
              "clock init");
+    if (mc_status st = exchange_ghosts(a, Q, s)) {
+        return st;
+    }
     StageParams p = fwd_params(a);
     p.q_in = Q;
     MCA_CUDA(mc::launch_cfl_min(p, 2, s), "cfl");
+    if (mc_status st = reduce_cfl_word(a, s)) {
+        return st;
+    }
     MCA_CUDA(mc::launch_record_clock(a->blk, 1, a->dts, a->mins, a->clamped, 0, s), "clock");
     for (int64_t n = 0; n < n_steps; ++n) {
         if (n % a->k == 0) {
@@ -621,6 +819,9 @@ mc_status mc_adjoint_forward(mc_adjoint* a, double* Q, const mc_clock* clock, in
             return st;
         }
         if (mc_status st = fwd_stage(a, a->work_b, Q, Q, mc::kSsp3Final, 1, dt, s)) {
+            return st;
+        }
+        if (mc_status st = reduce_cfl_word(a, s)) {
             return st;
         }
         MCA_CUDA(mc::launch_record_clock(a->blk, 0, a->dts, a->mins, a->clamped, n + 1, s), "clock");
@@ -689,10 +890,25 @@ mc_status mc_adjoint_backward(mc_adjoint* a, double* lambda, double* dgamma, voi
             MCA_CUDA(mc::launch_cfl_argmin(q0, a->nx, a->ny, a->grid.ng, a->grid.xc, a->grid.yc, a->scheme.gamma,
                                            a->grid.dx, a->mins + n0 + j, a->argmin, s),
                      "arg-min");
+            argmin_key_kernel<<<1, 1, 0, s>>>(a->argmin, a->rank, a->key);
+            if (a->sliced) {
+                // the lowest global arg-min cell and the step's whole dt sensitivity
+                if (mc_status st = comm_reduce(a, MC_COMM_MIN_I64, a->key, s)) {
+                    return st;
+                }
+                if (mc_status st = comm_reduce(a, MC_COMM_SUM_F64, a->scal, s)) {
+                    return st;
+                }
+            }
             dt_vjp_kernel<<<1, 1, 0, s>>>(q0, a->nx, a->grid.ng, a->grid.xc, a->grid.yc, a->scheme.gamma,
-                                          a->grid.dx, a->scheme.max_cfl, a->argmin, a->clamped + n0 + j, a->scal,
-                                          L3, a->scal + 1);
+                                          a->grid.dx, a->scheme.max_cfl, a->key, a->rank, a->clamped + n0 + j,
+                                          a->scal, L3, a->scal + 1);
             MCA_CUDA(cudaGetLastError(), "dt vjp");
+        }
+    }
+    if (a->sliced) {
+        if (mc_status st = comm_reduce(a, MC_COMM_SUM_F64, a->scal + 1, s)) {
+            return st;
         }
     }
     MCA_CUDA(cudaMemcpyAsync(lambda, L3, sb, cudaMemcpyDeviceToDevice, s), "lambda out");
@@ -700,6 +916,41 @@ mc_status mc_adjoint_backward(mc_adjoint* a, double* lambda, double* dgamma, voi
         MCA_CUDA(cudaMemcpyAsync(dgamma, a->scal + 1, sizeof(double), cudaMemcpyDeviceToHost, s), "dgamma");
         MCA_CUDA(cudaStreamSynchronize(s), "sync");
     }
+    return MC_OK;
+}
+
+mc_status mc_adjoint_set_slab_decomposition(mc_adjoint* a, const uint8_t* id, int32_t rank, int32_t world) {
+    if (!id) {
+        return afail(MC_ERR_INVALID_ARGUMENT, "null id");
+    }
+    if (mc_status st = slab_prepare(a, rank, world)) {
+        return st;
+    }
+    const char* why = "";
+    mc::SlabExchange* x = mc::slab_create(id, rank, world, 1, a->ny, a->grid.ng, a->grid.xc, a->grid.yc, 1, 4,
+                                          true, &why);
+    if (!x) {
+        return afail(MC_ERR_CUDA, std::string("slab communicator: ") + why);
+    }
+    a->slab = x;
+    a->rank = rank;
+    a->world = world;
+    a->sliced = true;
+    return MC_OK;
+}
+
+mc_status mc_adjoint_set_slab_hook(mc_adjoint* a, mc_comm_fn fn, void* user, int32_t rank, int32_t world) {
+    if (!fn) {
+        return afail(MC_ERR_INVALID_ARGUMENT, "null hook");
+    }
+    if (mc_status st = slab_prepare(a, rank, world)) {
+        return st;
+    }
+    a->comm_fn = fn;
+    a->comm_user = user;
+    a->rank = rank;
+    a->world = world;
+    a->sliced = true;
     return MC_OK;
 }
 

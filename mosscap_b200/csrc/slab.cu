@@ -203,4 +203,50 @@ cudaError_t slab_reduce_min(SlabExchange* s, uint64_t* word, cudaStream_t stream
     return cudaSuccess;
 }
 
+cudaError_t slab_halo(SlabExchange* s, const double* send_lo, const double* send_hi, double* recv_lo,
+                      double* recv_hi, size_t count, cudaStream_t stream, const char** err) {
+    const NcclApi& a = *s->api;
+    // down first, then up, as in slab_exchange
+    ncclResult_t r = a.group_start();
+    if (r == ncclSuccess && s->below >= 0) {
+        r = a.send(send_lo, count, ncclFloat64, s->below, s->comm, stream);
+    }
+    if (r == ncclSuccess && s->above >= 0) {
+        r = a.recv(recv_hi, count, ncclFloat64, s->above, s->comm, stream);
+    }
+    if (r == ncclSuccess && s->above >= 0) {
+        r = a.send(send_hi, count, ncclFloat64, s->above, s->comm, stream);
+    }
+    if (r == ncclSuccess && s->below >= 0) {
+        r = a.recv(recv_lo, count, ncclFloat64, s->below, s->comm, stream);
+    }
+    const ncclResult_t r2 = a.group_end();
+    if (r == ncclSuccess) {
+        r = r2;
+    }
+    if (r != ncclSuccess) {
+        *err = a.error_string(r);
+        return cudaErrorUnknown;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t slab_all_reduce(SlabExchange* s, void* buf, size_t count, SlabReduce op, cudaStream_t stream,
+                            const char** err) {
+    ncclDataType_t type = ncclUint64;
+    ncclRedOp_t red = ncclMin;
+    if (op == SlabReduce::kSumF64) {
+        type = ncclFloat64;
+        red = ncclSum;
+    } else if (op == SlabReduce::kMinI64) {
+        type = ncclInt64;
+    }
+    const ncclResult_t r = s->api->all_reduce(buf, buf, count, type, red, s->comm, stream);
+    if (r != ncclSuccess) {
+        *err = s->api->error_string(r);
+        return cudaErrorUnknown;
+    }
+    return cudaSuccess;
+}
+
 } // namespace mc

@@ -41,4 +41,16 @@ cudaError_t slab_exchange(SlabExchange* s, double* q, cudaStream_t stream, const
 // of this rank's non-negative CFL minimum (integer order = value order).
 cudaError_t slab_reduce_min(SlabExchange* s, uint64_t* word, cudaStream_t stream, const char** err);
 
+// Enqueue on `stream` one exchange of contiguous blocks of `count` doubles
+// with the neighbours along the slab axis: send_lo goes to the rank below
+// (into its recv_hi), send_hi to the rank above (into its recv_lo). A side
+// with no neighbour sends and receives nothing.
+cudaError_t slab_halo(SlabExchange* s, const double* send_lo, const double* send_hi, double* recv_lo,
+                      double* recv_hi, size_t count, cudaStream_t stream, const char** err);
+
+// In-place all-reduce of `count` elements over the ranks, in `stream`.
+enum class SlabReduce { kMinU64, kSumF64, kMinI64 };
+cudaError_t slab_all_reduce(SlabExchange* s, void* buf, size_t count, SlabReduce op, cudaStream_t stream,
+                            const char** err);
+
 } // namespace mc

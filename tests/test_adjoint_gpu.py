@@ -184,3 +184,23 @@ def test_adjoint_matches_gpu_tangent_linear(gpu_lib):
     for k in range(8):
         ad = float((gvy * dirs[k]).sum()) + gg * dgs[k]
         assert abs(ad - dJ[k]) / abs(dJ[k]) < 1e-9, (k, ad, dJ[k])
+
+
+def test_adjoint_zero_steps_is_identity(gpu_lib):
+    """A recorded run of 0 steps leaves the state alone and its reverse sweep
+    returns the cotangent unchanged with dJ/dgamma = 0."""
+    from mosscap_b200.adjoint import _Runner, pad_periodic
+    p = P.kelvin_helmholtz_2d(32, seed=0)
+    ng = p.ng
+    q0 = torch.tensor(p.Q[:, 0, ng:-ng, ng:-ng], dtype=torch.float64, device="cuda")
+    qpad = pad_periodic(q0, ng)
+    before = qpad.clone()
+    runner = _Runner(p, p.gamma, 4)
+    runner.forward(qpad, 0)
+    lam = torch.randn(qpad.shape, generator=torch.Generator().manual_seed(5), dtype=torch.float64).cuda()
+    lam_in = lam.clone()
+    dg = runner.backward(lam)
+    torch.cuda.synchronize()
+    assert torch.equal(qpad, before)
+    assert torch.equal(lam, lam_in)
+    assert dg == 0.0

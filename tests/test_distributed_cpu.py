@@ -127,3 +127,68 @@ def test_partition_by_cost_balances_the_batch(world):
     loads = [sum(costs[k] for k in part) for part in parts]
     assert max(loads) <= sum(costs) / world + max(costs)
     assert max(loads) / (sum(costs) / world) < 1.02
+
+
+def _comm_worker(rank, world, port, errors):
+    from mosscap_b200 import capi
+    from mosscap_b200.adjoint import comm_op
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        count = 6
+        # rank r sends its first rows (send_lo) down and its last rows up
+        send_lo = torch.full((count,), 100.0 * rank + 1, dtype=torch.float64)
+        send_hi = torch.full((count,), 100.0 * rank + 2, dtype=torch.float64)
+        recv_lo = torch.zeros(count, dtype=torch.float64)
+        recv_hi = torch.zeros(count, dtype=torch.float64)
+        comm_op(capi.COMM_HALO, (send_lo, send_hi, recv_lo, recv_hi), rank, world, via_host=True)
+        below, above = (rank - 1) % world, (rank + 1) % world
+        # from below: its last rows; from above: its first rows
+        if not torch.all(recv_lo == 100.0 * below + 2) or not torch.all(recv_hi == 100.0 * above + 1):
+            errors.put(f"rank {rank}: halo {recv_lo[0].item()} {recv_hi[0].item()}")
+        key = torch.tensor([0x7FFFFFFFFFFFFFFF if rank == 0 else (rank << 32) | (7 - rank)], dtype=torch.int64)
+        comm_op(capi.COMM_MIN_I64, (key,), rank, world, via_host=True)
+        if key.item() != ((1 << 32) | 6):
+            errors.put(f"rank {rank}: arg-min key {key.item():#x}")
+        s = torch.tensor([0.5 * (rank + 1)], dtype=torch.float64)
+        comm_op(capi.COMM_SUM_F64, (s,), rank, world, via_host=True)
+        if s.item() != 0.25 * world * (world + 1):
+            errors.put(f"rank {rank}: sum {s.item()}")
+        bits = torch.tensor([np.float64(1.0 + rank).view(np.int64)], dtype=torch.int64)
+        comm_op(capi.COMM_MIN_U64, (bits,), rank, world, via_host=True)
+        if np.int64(bits.item()).view(np.float64) != 1.0:
+            errors.put(f"rank {rank}: min {bits.item()}")
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_adjoint_slab_comm_hook_gloo(world):
+    """The adjoint's slab hook operations (adjoint.comm_op) between gloo
+    ranks: halo blocks travel to the ring neighbours (periodic, y order), the
+    arg-min key reduces to the lowest rank holding a cell, sums and the
+    double-bits minimum reduce in place."""
+    ctx = mp.get_context("spawn")
+    errors = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_comm_worker, args=(r, world, port, errors)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert errors.empty(), errors.get()
+
+
+def test_adjoint_slab_comm_hook_single_rank():
+    """One rank is its own periodic neighbour; reductions are identities."""
+    from mosscap_b200 import capi
+    from mosscap_b200.adjoint import comm_op
+    a, b = torch.arange(4.0, dtype=torch.float64), torch.arange(4.0, 8.0, dtype=torch.float64)
+    lo, hi = torch.zeros(4, dtype=torch.float64), torch.zeros(4, dtype=torch.float64)
+    comm_op(capi.COMM_HALO, (a, b, lo, hi), 0, 1)
+    assert torch.equal(lo, b) and torch.equal(hi, a)
+    s = torch.tensor([3.0], dtype=torch.float64)
+    comm_op(capi.COMM_SUM_F64, (s,), 0, 1)
+    assert s.item() == 3.0
