@@ -454,8 +454,9 @@ def run_sedov(args):
 
 
 def measure_batch(problems, precision, steps, warmup, tune=True):
-    """Batched independent problems (one persistent launch per stage kind,
-    graph-replayed steps, autotuned schedule); returns a dict."""
+    """Batched independent problems (one persistent launch per stage, or
+    the split form where the autotuner measures it faster; graph-replayed
+    steps, autotuned schedule); returns a dict."""
     import torch
     from mosscap_b200.hydro import BatchSim
     cells = sum(p.interior_cells for p in problems)

@@ -291,8 +291,10 @@ mc_status mc_stage_time(mc_ctx* ctx, int32_t kind, double* total_ms, int64_t* la
  *
  * Thousands of independent 1D / 2D problems of uneven size advance together:
  * every step of the whole batch is one persistent kernel launch per SSPRK
- * stage (all problems' tiles in one work list) plus one clock launch, and the
- * step is replayed from a captured CUDA graph. Each problem runs the
+ * stage (the 2D problems' tiles and the 1D problems' warp tasks in one work
+ * list) plus one clock launch, and the step is replayed from a captured CUDA
+ * graph. (The autotuner may instead split each stage into a launch over the
+ * tiles and one over the 1D tasks, when that measures more than 2 % faster.) Each problem runs the
  * reference's main loop on its own (source/main.cpp:54-72): its own CFL dt,
  * clamped to its own output times and max_time; outputs only advance its
  * clock (prev_output_time = time); a problem that reaches max_time stops.
@@ -315,12 +317,13 @@ mc_status mc_batch_create(const mc_batch_problem* problems, int32_t n, const mc_
 mc_status mc_batch_destroy(mc_batch* batch);
 /* Fill every problem's ghost cells (fill_bcs per problem). */
 mc_status mc_batch_fill_bcs(mc_batch* batch, double* pool, void* stream);
-/* Autotuner: times the stage kernels (one launch over the 2D problems'
- * tiles, one over the 1D problems' warp tasks) on this pool for every
- * candidate schedule (persistent grid size, static or dynamic work
- * distribution; for the 1D launch also the segments per warp task) with CUDA
- * events and keeps the fastest of each. Leaves the pool unchanged. Waits for
- * the stream. */
+/* Autotuner: times a stage on this pool with CUDA events in both forms (one
+ * launch over all work items; a launch over the 2D problems' tiles plus one
+ * over the 1D problems' warp tasks) for every candidate schedule (persistent
+ * grid size, static or dynamic work distribution, segments per 1D warp task)
+ * and keeps the fastest schedule of each form, and the one-launch form
+ * unless the split form is more than 2 % faster. Leaves the pool unchanged.
+ * Waits for the stream. */
 mc_status mc_batch_tune(mc_batch* batch, double* pool, void* stream);
 /* Up to `steps` steps of every unfinished problem, each with its own dt, on
  * the device (graph replay). The first call computes every problem's first
@@ -330,8 +333,14 @@ mc_status mc_batch_advance(mc_batch* batch, double* pool, int64_t steps, void* s
  * Waits for the stream. */
 mc_status mc_batch_clocks(mc_batch* batch, mc_clock* clocks, int64_t* steps, uint32_t* status, void* stream);
 /* The schedule in use: grid size in CTAs and 1 if dynamic, of the launch over
- * the 2D tiles; 1D segments per warp task. */
+ * all work items (one launch per stage) or of the launch over the 2D tiles
+ * (two); 1D segments per warp task. */
 mc_status mc_batch_schedule(const mc_batch* batch, int32_t* grid, int32_t* dynamic, int32_t* segs_per_task);
+/* Launches per stage: 1 (the default: one launch over all work items) or 2
+ * (the tiles, then the 1D tasks). The setter overrides the autotuner's
+ * choice until the next mc_batch_tune. */
+mc_status mc_batch_set_stage_launches(mc_batch* batch, int32_t launches);
+mc_status mc_batch_stage_launches(const mc_batch* batch, int32_t* launches);
 
 /* ---- Discrete adjoint --------------------------------------------------------
  *

@@ -157,6 +157,10 @@ def load() -> ctypes.CDLL:
     lib.mc_batch_clocks.restype = i32
     lib.mc_batch_schedule.argtypes = [vp, P(i32), P(i32), P(i32)]
     lib.mc_batch_schedule.restype = i32
+    lib.mc_batch_set_stage_launches.argtypes = [vp, i32]
+    lib.mc_batch_set_stage_launches.restype = i32
+    lib.mc_batch_stage_launches.argtypes = [vp, P(i32)]
+    lib.mc_batch_stage_launches.restype = i32
     lib.mc_time_step_noalloc.argtypes = [P(McGrid), P(McScheme), vp, d, vp]
     lib.mc_time_step_noalloc.restype = i32
     lib.mc_set_cfl_reduce_hook.argtypes = [vp, CFL_REDUCE_FN, vp]

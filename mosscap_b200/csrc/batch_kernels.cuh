@@ -1,14 +1,16 @@
 // Batched stage kernels: persistent launches advance one SSPRK stage of
 // every problem of a batch of independent 1D and 2D problems of uneven size.
 //
-// Two work lists, one kernel each (PART): the 2D tiles (one CTA each, the
-// tile2d body of the single-problem kernel) and bundles of kWarps 1D tasks
-// (one warp each, a task being `nseg` consecutive 30-cell segments of one 1D
-// problem, the segment1d body), so the warps of one CTA may serve different
-// small problems. Keeping the two bodies in separate kernels keeps each
-// kernel's instruction footprint that of one body. CTAs take work items
-// either statically (item = blockIdx.x + k * gridDim.x) or dynamically from
-// an atomic counter; the autotuner picks. Every problem has its own
+// Two kinds of work item: a 2D tile (one CTA, the tile2d body of the
+// single-problem kernel) and a bundle of 1D tasks, one per warp of the CTA
+// (a task being `nseg` consecutive 30-cell segments of one 1D problem, the
+// segment1d body), so the warps of one CTA may serve different small
+// problems. PART kPartAll runs both in one persistent launch per stage: its
+// work list is the 2D tiles, biggest problems first, then the 1D bundles.
+// PARTs kPart2d and kPart1d split them into two launches, each kernel with
+// the instruction footprint of one body; the autotuner picks the form. CTAs
+// take work items either statically (item = blockIdx.x + k * gridDim.x) or
+// dynamically from an atomic counter. Every problem has its own
 // DeviceBlock: its dt, clock, CFL-minimum cell and status, so each problem
 // advances with its own dt.
 #pragma once
@@ -32,19 +34,15 @@ struct BatchStageParams {
     int n2d;
     const BatchTask1d* tasks1d;
     int ntasks1d;
-    int n_items;                // work items of this launch: n2d tiles, or bundles of kWarps 1D tasks
+    int n_items;                // work items of this launch: the tiles, the 1D bundles or both
     int dynamic;
     int* counter;               // work counter of this launch (dynamic schedule)
 };
 
-constexpr int kPart2d = 0;  // the launch over the 2D tiles
-constexpr int kPart1d = 1;  // the launch over the 1D task bundles
+constexpr int kPart2d = 0;   // the launch over the 2D tiles
+constexpr int kPart1d = 1;   // the launch over the 1D task bundles
+constexpr int kPartAll = 2;  // one launch over both
 
-template <int REC, class T, int PART>
-__host__ __device__ constexpr size_t batch_smem_bytes() {
-    // a 2D tile of 4 variables, or kWarps 1D windows of 3 variables
-    return PART == kPart2d ? smem_bytes<2, REC, T>(4) : smem_bytes<1, REC, T>(3);
-}
 
 // CTAs per SM of the batched kernels: the per-problem parameters come from
 // global memory rather than the constant bank, so the tile body needs more
@@ -52,11 +50,69 @@ __host__ __device__ constexpr size_t batch_smem_bytes() {
 // with up to 128 registers measured 7 % faster than three with 80).
 constexpr int kMinBlocksBatch = 2;
 // Threads per CTA: the 2D tiles run 320 (ten warps, three of a pass's 30
-// lines each; 24 % faster than 256 on the 4096-problem set), the 1D bundles
-// one task per warp of 256.
+// lines each; 24 % faster than 256 on the 4096-problem set), so the merged
+// kernel does too (bundles of ten 1D tasks); the 1D kernel alone runs one
+// task per warp of 256.
 template <int PART>
 __host__ __device__ constexpr int batch_threads() {
-    return PART == kPart2d ? 320 : kThreads;
+    return PART == kPart1d ? kThreads : 320;
+}
+// 1D tasks per bundle: one per warp.
+template <int PART>
+__host__ __device__ constexpr int batch_warps() {
+    return batch_threads<PART>() / 32;
+}
+
+template <int REC, class T, int PART>
+__host__ __device__ constexpr size_t batch_smem_bytes() {
+    // a 2D tile of 4 variables and / or one 1D window of 3 variables per warp
+    constexpr size_t tile = smem_bytes<2, REC, T>(4);
+    constexpr size_t windows = sizeof(T) * 3 * (size_t)batch_warps<PART>() * seg1d_window<REC>();
+    return PART == kPart2d ? tile : PART == kPart1d ? windows : (tile > windows ? tile : windows);
+}
+
+template <int REC, int LIM, int RS, class T, int NT>
+__device__ __forceinline__ void batch_tile(const BatchStageParams& bp, int item, T* smem, double* red_d,
+                                           unsigned* red_u) {
+    // the problem's parameters, bound to this stage's buffers, are read in
+    // place from global memory
+    const BatchItem2d it = bp.items2d[item];
+    const StageParams& p = bp.probs[it.prob];
+    if (!p.blk->done) {
+        double dtmin = __longlong_as_double((long long)kInfBits);
+        unsigned flags = 0;
+        tile2d<2, REC, LIM, RS, T, false, NT>(p, it.bx, it.by, 0, smem, dtmin, flags);
+        block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
+    }
+}
+
+template <int REC, int LIM, int RS, class T, int NW>
+__device__ __forceinline__ void batch_bundle(const BatchStageParams& bp, int bundle, T* smem) {
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int t = bundle * NW + warp;
+    if (t < bp.ntasks1d) {
+        const BatchTask1d task = bp.tasks1d[t];
+        const StageParams& p = bp.probs[task.prob];
+        if (!p.blk->done) {
+            double dtmin = __longlong_as_double((long long)kInfBits);
+            unsigned flags = 0;
+            T* W = smem + (size_t)warp * 3 * seg1d_window<REC>();
+            for (int s = 0; s < task.nseg; ++s) {
+                segment1d<REC, LIM, RS, T>(p, (task.s0 + s) * kTile, W, dtmin, flags);
+            }
+            dtmin = warp_min(dtmin);
+            flags = warp_or(flags);
+            if (lane == 0) {
+                if (p.last) {
+                    atomicMin(&p.blk->cfl_min_bits, ordered_bits(dtmin));
+                }
+                if (flags) {
+                    atomicOr(&p.blk->status, flags);
+                }
+            }
+        }
+    }
 }
 
 template <int REC, int LIM, int RS, class T, int PART>
@@ -66,8 +122,7 @@ __global__ void __launch_bounds__(batch_threads<PART>(), kMinBlocksBatch) batch_
     __shared__ unsigned red_u[batch_threads<PART>() / 32];
     __shared__ int s_item;
     T* smem = reinterpret_cast<T*>(smem_raw);
-    const int warp = threadIdx.x >> 5;
-    const int lane = threadIdx.x & 31;
+    constexpr int NT = batch_threads<PART>();
     int item = blockIdx.x;
     for (;;) {
         if (bp.dynamic) {
@@ -81,40 +136,13 @@ __global__ void __launch_bounds__(batch_threads<PART>(), kMinBlocksBatch) batch_
             break;
         }
         if constexpr (PART == kPart2d) {
-            // the problem's parameters, bound to this stage's buffers, are
-            // read in place from global memory
-            const BatchItem2d it = bp.items2d[item];
-            const StageParams& p = bp.probs[it.prob];
-            if (!p.blk->done) {
-                double dtmin = __longlong_as_double((long long)kInfBits);
-                unsigned flags = 0;
-                tile2d<2, REC, LIM, RS, T, false, batch_threads<PART>()>(p, it.bx, it.by, 0, smem, dtmin, flags);
-                block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
-            }
+            batch_tile<REC, LIM, RS, T, NT>(bp, item, smem, red_d, red_u);
+        } else if constexpr (PART == kPart1d) {
+            batch_bundle<REC, LIM, RS, T, batch_warps<PART>()>(bp, item, smem);
+        } else if (item < bp.n2d) {
+            batch_tile<REC, LIM, RS, T, NT>(bp, item, smem, red_d, red_u);
         } else {
-            const int t = item * kWarps + warp;
-            if (t < bp.ntasks1d) {
-                const BatchTask1d task = bp.tasks1d[t];
-                const StageParams& p = bp.probs[task.prob];
-                if (!p.blk->done) {
-                    double dtmin = __longlong_as_double((long long)kInfBits);
-                    unsigned flags = 0;
-                    T* W = smem + (size_t)warp * 3 * seg1d_window<REC>();
-                    for (int s = 0; s < task.nseg; ++s) {
-                        segment1d<REC, LIM, RS, T>(p, (task.s0 + s) * kTile, W, dtmin, flags);
-                    }
-                    dtmin = warp_min(dtmin);
-                    flags = warp_or(flags);
-                    if (lane == 0) {
-                        if (p.last) {
-                            atomicMin(&p.blk->cfl_min_bits, ordered_bits(dtmin));
-                        }
-                        if (flags) {
-                            atomicOr(&p.blk->status, flags);
-                        }
-                    }
-                }
-            }
+            batch_bundle<REC, LIM, RS, T, batch_warps<PART>()>(bp, item - bp.n2d, smem);
         }
         __syncthreads();
         if (!bp.dynamic) {

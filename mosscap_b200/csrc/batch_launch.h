@@ -7,8 +7,8 @@
 
 namespace mc {
 
-// Launch one part (kPart2d: the 2D tiles, kPart1d: the 1D task bundles) of
-// one batched stage on `grid` CTAs; with occupancy != NULL, only report the
+// Launch one part (kPart2d: the 2D tiles, kPart1d: the 1D task bundles,
+// kPartAll: both) of one batched stage on `grid` CTAs; with occupancy != NULL, only report the
 // resident CTAs per SM of that kernel instead.
 cudaError_t launch_batch_stage_fp64(const BatchStageParams& bp, int rec, int lim, int rs, int part, int grid,
                                     cudaStream_t s, int* occupancy);

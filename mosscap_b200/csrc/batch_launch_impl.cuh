@@ -34,8 +34,14 @@ cudaError_t launch_batch_part(const BatchStageParams& bp, int grid, cudaStream_t
 
 template <int REC, int LIM, int RS>
 cudaError_t launch_batch_one(const BatchStageParams& bp, int part, int grid, cudaStream_t s, int* occupancy) {
-    return part == kPart2d ? launch_batch_part<REC, LIM, RS, kPart2d>(bp, grid, s, occupancy)
-                           : launch_batch_part<REC, LIM, RS, kPart1d>(bp, grid, s, occupancy);
+    switch (part) {
+        case kPart2d:
+            return launch_batch_part<REC, LIM, RS, kPart2d>(bp, grid, s, occupancy);
+        case kPart1d:
+            return launch_batch_part<REC, LIM, RS, kPart1d>(bp, grid, s, occupancy);
+        default:
+            return launch_batch_part<REC, LIM, RS, kPartAll>(bp, grid, s, occupancy);
+    }
 }
 
 template <int REC, int LIM>

@@ -333,7 +333,15 @@ class BatchSim:
         g, d, s = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         capi.check(self.lib.mc_batch_schedule(self.ctx, ctypes.byref(g), ctypes.byref(d), ctypes.byref(s)),
                    "mc_batch_schedule")
-        return {"grid": g.value, "dynamic": bool(d.value), "segments_per_task": s.value}
+        n = ctypes.c_int32()
+        capi.check(self.lib.mc_batch_stage_launches(self.ctx, ctypes.byref(n)), "mc_batch_stage_launches")
+        return {"grid": g.value, "dynamic": bool(d.value), "segments_per_task": s.value,
+                "launches_per_stage": n.value}
+
+    def set_stage_launches(self, n: int) -> None:
+        """1: one launch per stage over all work items; 2: the 2D tiles and
+        the 1D tasks in separate launches (until the next tune())."""
+        capi.check(self.lib.mc_batch_set_stage_launches(self.ctx, int(n)), "mc_batch_set_stage_launches")
 
     def advance(self, steps: int) -> None:
         capi.check(self.lib.mc_batch_advance(self.ctx, self._pool(), int(steps), self._stream()), "mc_batch_advance")

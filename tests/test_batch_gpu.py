@@ -1,6 +1,7 @@
 """GPU tests of the batched form (mc_batch_*): independent 1D and 2D Riemann
-problems of uneven size advanced by one persistent launch per stage, each
-with its own dt, replayed from a CUDA graph.
+problems of uneven size advanced by one persistent launch per stage (or, in
+the split form, one over the 2D tiles and one over the 1D tasks), each with
+its own dt, replayed from a CUDA graph.
 
 Every problem must match the reference algorithm (the oracle, run on that
 problem alone) bit for bit while its state stays finite; the seeded set
@@ -73,6 +74,26 @@ def test_batch_schedule_independent(gpu_lib):
     assert np.array_equal(_bits(ta), _bits(tb)), (sched_a, sched_b)
     for k in range(len(probs)):
         assert np.array_equal(_bits(a.get_Q(k)), _bits(b.get_Q(k))), (k, sched_a, sched_b)
+
+
+def test_batch_one_and_two_launches_per_stage_agree(gpu_lib):
+    """One launch per stage over the 2D tiles and the 1D tasks together (the
+    default) and the split form give bit-identical states and clocks."""
+    from mosscap_b200.hydro import BatchSim
+    probs = _small_batch("hllc", seed=13)
+    runs = []
+    for n in (1, 2):
+        b = BatchSim(probs)
+        b.set_stage_launches(n)
+        assert b.schedule()["launches_per_stage"] == n
+        b.fill_bcs()
+        b.advance(8)
+        runs.append(b)
+    ta, _, _ = runs[0].clocks()
+    tb, _, _ = runs[1].clocks()
+    assert np.array_equal(_bits(ta), _bits(tb))
+    for k in range(len(probs)):
+        assert np.array_equal(_bits(runs[0].get_Q(k)), _bits(runs[1].get_Q(k))), k
 
 
 def test_batch_output_clamp_and_max_time(gpu_lib, oracle_port):
