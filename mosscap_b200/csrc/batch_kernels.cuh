@@ -74,10 +74,19 @@ __host__ __device__ constexpr size_t batch_smem_bytes() {
 template <int REC, int LIM, int RS, class T, int NT>
 __device__ __forceinline__ void batch_tile(const BatchStageParams& bp, int item, T* smem, double* red_d,
                                            unsigned* red_u) {
-    // the problem's parameters, bound to this stage's buffers, are read in
-    // place from global memory
+    // the problem's parameters, bound to this stage's buffers, copied once
+    // per tile into shared memory
+    __shared__ StageParams s_p;
     const BatchItem2d it = bp.items2d[item];
-    const StageParams& p = bp.probs[it.prob];
+    {
+        const int* src = reinterpret_cast<const int*>(&bp.probs[it.prob]);
+        int* dst = reinterpret_cast<int*>(&s_p);
+        for (int k = threadIdx.x; k < (int)(sizeof(StageParams) / 4); k += NT) {
+            dst[k] = src[k];
+        }
+    }
+    __syncthreads();
+    const StageParams& p = s_p;
     if (!p.blk->done) {
         double dtmin = __longlong_as_double((long long)kInfBits);
         unsigned flags = 0;
