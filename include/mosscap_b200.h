@@ -294,7 +294,7 @@ mc_status mc_stage_time(mc_ctx* ctx, int32_t kind, double* total_ms, int64_t* la
  * stage (the 2D problems' tiles and the 1D problems' warp tasks in one work
  * list) plus one clock launch, and the step is replayed from a captured CUDA
  * graph. (The autotuner may instead split each stage into a launch over the
- * tiles and one over the 1D tasks, when that measures more than 2 % faster.) Each problem runs the
+ * tiles and one over the 1D tasks, when that measures more than 5 % faster.) Each problem runs the
  * reference's main loop on its own (source/main.cpp:54-72): its own CFL dt,
  * clamped to its own output times and max_time; outputs only advance its
  * clock (prev_output_time = time); a problem that reaches max_time stops.
@@ -322,7 +322,7 @@ mc_status mc_batch_fill_bcs(mc_batch* batch, double* pool, void* stream);
  * over the 1D problems' warp tasks) for every candidate schedule (persistent
  * grid size, static or dynamic work distribution, segments per 1D warp task)
  * and keeps the fastest schedule of each form, and the one-launch form
- * unless the split form is more than 2 % faster. Leaves the pool unchanged.
+ * unless the split form is more than 5 % faster. Leaves the pool unchanged.
  * Waits for the stream. */
 mc_status mc_batch_tune(mc_batch* batch, double* pool, void* stream);
 /* Up to `steps` steps of every unfinished problem, each with its own dt, on
