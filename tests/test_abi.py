@@ -57,3 +57,23 @@ def test_enum_values_are_reference_ordinals():
                       ("MC_STEPPER_SSPRK4", 2), ("MC_BC_ZEROGRAD", 4), ("MC_BC_USERFN", 6)]:
         assert f"{name} = {val}" in text
     assert capi.RECON["weno5z"] == 3 and capi.BOUNDARY["constant"] == 5
+
+
+def test_slab_and_batch_form_entry_points_reject_bad_arguments():
+    """Argument checks of the adjoint's slab entry points and the batch's
+    launch-form switch, which fail before any device call."""
+    lib = capi.load()
+    INVALID = 1  # MC_ERR_INVALID_ARGUMENT
+    assert capi.STATUS_NAMES[INVALID] == "MC_ERR_INVALID_ARGUMENT"
+    hook = capi.COMM_FN(lambda user, op, bufs, count, stream: 0)
+    uid = ctypes.create_string_buffer(128)
+    assert lib.mc_adjoint_set_slab_hook(None, hook, None, 0, 1) == INVALID
+    assert lib.mc_adjoint_set_slab_decomposition(None, uid, 0, 1) == INVALID
+    assert lib.mc_batch_set_stage_launches(None, 1) == INVALID
+    n = ctypes.c_int32()
+    assert lib.mc_batch_stage_launches(None, ctypes.byref(n)) == INVALID
+    # the hook operation codes are the header's
+    text = open(capi.HEADER).read()
+    for name, val in [("MC_COMM_HALO", capi.COMM_HALO), ("MC_COMM_MIN_U64", capi.COMM_MIN_U64),
+                      ("MC_COMM_SUM_F64", capi.COMM_SUM_F64), ("MC_COMM_MIN_I64", capi.COMM_MIN_I64)]:
+        assert f"{name} = {val}" in text
