@@ -395,6 +395,11 @@ def run_ours(args):
         if extras is not None:
             line["forms"] = extras
         print(json.dumps(line), flush=True)
+    if slab is not None:
+        # the library's own NCCL communicator goes first, on every rank, with
+        # no work in flight, and only then torch's process group
+        torch.cuda.synchronize(dev)
+        slab.sim.close()
     del sim
     if world > 1:
         dist.destroy_process_group()
