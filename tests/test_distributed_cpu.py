@@ -192,3 +192,17 @@ def test_adjoint_slab_comm_hook_single_rank():
     s = torch.tensor([3.0], dtype=torch.float64)
     comm_op(capi.COMM_SUM_F64, (s,), 0, 1)
     assert s.item() == 3.0
+
+
+def test_slab_adjoint_rejects_bad_partitions_on_the_host():
+    """SlabAdjoint checks its partition before touching the device: the rows
+    must divide by the ranks, the problem must be 2D and the transport known."""
+    from mosscap_b200 import problems as P
+    from mosscap_b200.adjoint import SlabAdjoint
+    p = P.kelvin_helmholtz_2d(30, seed=0)
+    with pytest.raises(ValueError):
+        SlabAdjoint(p, p.gamma, rank=0, world=4)
+    with pytest.raises(ValueError):
+        SlabAdjoint(p, p.gamma, rank=0, world=2, transport="carrier-pigeon")
+    with pytest.raises(ValueError):
+        SlabAdjoint(P.sod_1d(64), 1.4)
