@@ -180,6 +180,12 @@ mc_status mc_set_cfl_reduce_hook(mc_ctx* ctx, void (*fn)(void* user, uint64_t* c
  * No counterpart in the reference, which runs one domain. */
 mc_status mc_slab_unique_id(uint8_t* id /* 128 bytes */);
 mc_status mc_set_slab_decomposition(mc_ctx* ctx, const uint8_t* id, int32_t rank, int32_t world);
+/* 2D slabs (on by default): each stage runs as two launches, the tile rows
+ * that read ghost rows or write the layers that are sent, and the other
+ * rows on a second internal stream, and the exchange of the first runs
+ * beside the second; the next stage's border rows wait for it. Same results
+ * either way. Not taken with a non-ideal EOS or a user boundary hook. */
+mc_status mc_set_slab_overlap(mc_ctx* ctx, int32_t enable);
 
 /* ---- Non-ideal equations of state --------------------------------------------
  *

@@ -135,6 +135,8 @@ def load() -> ctypes.CDLL:
     lib.mc_slab_unique_id.restype = i32
     lib.mc_set_slab_decomposition.argtypes = [vp, ctypes.c_char_p, i32, i32]
     lib.mc_set_slab_decomposition.restype = i32
+    lib.mc_set_slab_overlap.argtypes = [vp, i32]
+    lib.mc_set_slab_overlap.restype = i32
     lib.mc_tangent_linear.argtypes = [P(McGrid), P(McScheme), vp, vp, P(d), i32, P(McClock), i64, vp]
     lib.mc_tangent_linear.restype = i32
     lib.mc_get_status.argtypes = [vp, P(ctypes.c_uint32), vp]

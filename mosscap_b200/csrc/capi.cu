@@ -40,6 +40,16 @@ struct mc_ctx {
     void* cfl_hook_data = nullptr;
     mc::SlabExchange* slab = nullptr;  // mc_set_slab_decomposition
     int slab_faces = 0;                // faces whose ghosts the slab exchange fills
+    // 2D slabs: the exchange of a stage's border layers overlaps its interior
+    // tiles (mc_set_slab_overlap). Border tile rows [0, ov_b0) and
+    // [ov_b1, ov_rows) read ghost rows or write layers that are sent; they run
+    // on ov_border, their exchange on ov_comm, the interior rows on
+    // ov_interior, ordered by events; the caller's stream forks and joins.
+    bool slab_overlap = true;
+    int ov_b0 = 0, ov_b1 = 0, ov_rows = 0;
+    cudaStream_t ov_border = nullptr, ov_interior = nullptr, ov_comm = nullptr;
+    cudaEvent_t ov_fork = nullptr;
+    cudaEvent_t ov_border_done[4] = {}, ov_interior_done[4] = {}, ov_exch_done[4] = {};
     int gravity = 0;              // mc_set_gravity
     double grav[3] = {0.0, 0.0, 0.0};
     // non-ideal EOS (mc_set_eos)
@@ -59,6 +69,9 @@ struct mc_ctx {
     struct Timed {
         cudaEvent_t start, stop;
         int kind;
+        // an overlapped stage's second piece (null otherwise): the stage
+        // lasts from the first start to the last stop
+        cudaEvent_t start2, stop2;
     };
     std::vector<Timed> timed;
     std::vector<cudaEvent_t> event_pool;
@@ -136,7 +149,7 @@ cudaError_t launch_stage(mc_ctx* c, const StageParams& p, int pass, cudaStream_t
     if (!c->profiling) {
         return launch_stage_kernel(c, p, pass, s);
     }
-    mc_ctx::Timed t{pooled_event(c), pooled_event(c), c->grid.num_dim == 3 ? pass : 0};
+    mc_ctx::Timed t{pooled_event(c), pooled_event(c), c->grid.num_dim == 3 ? pass : 0, nullptr, nullptr};
     cudaEventRecord(t.start, s);
     const cudaError_t e = launch_stage_kernel(c, p, pass, s);
     cudaEventRecord(t.stop, s);
@@ -221,8 +234,15 @@ mc_status exchange_slab(mc_ctx* c, double* q, cudaStream_t s) {
     return MC_OK;
 }
 
+mc_status enqueue_step_overlapped(mc_ctx* c, double* Q, double dt, const double* dt_dev, bool reset_min,
+                                  cudaStream_t s);
+bool overlapped(const mc_ctx* c);
+
 // Enqueue one SSPRK step on Q. dt_dev (device-driven loop) or dt (host).
 mc_status enqueue_step(mc_ctx* c, double* Q, double dt, const double* dt_dev, bool reset_min, cudaStream_t s) {
+    if (overlapped(c)) {
+        return enqueue_step_overlapped(c, Q, dt, dt_dev, reset_min, s);
+    }
     const mc::StagePlan plan = mc::plan_for(c->scheme.time_stepper);
     double* bufs[3] = {Q, c->buf_a, c->buf_b};
     c->last_stage_in = bufs[plan.in[plan.n - 1]];
@@ -275,6 +295,85 @@ mc_status enqueue_step(mc_ctx* c, double* Q, double dt, const double* dt_dev, bo
     return MC_OK;
 }
 
+// Whether a step of this context runs with the slab exchange overlapping
+// the interior tiles.
+bool overlapped(const mc_ctx* c) {
+    return c->slab && c->slab_overlap && c->ov_border && c->grid.num_dim == 2 && c->eos_type == mc::kEosIdeal &&
+           !c->user_bc && c->ov_b0 < c->ov_b1;
+}
+
+// One SSPRK step of a 2D slab with each stage's exchange beside its
+// interior tiles. Per stage: the border tile rows (after the previous stage
+// and its exchange) on ov_border; the exchange of the layers they wrote on
+// ov_comm; the interior tile rows (after the previous stage's border rows;
+// its interior rows come earlier on the same stream) on ov_interior. The
+// interior rows neither read ghost rows nor write the layers that are sent,
+// and the exchange writes only ghost rows, so the pieces touch disjoint
+// cells; the result is that of enqueue_step. The caller's stream waits for
+// the last stage and its exchange.
+mc_status enqueue_step_overlapped(mc_ctx* c, double* Q, double dt, const double* dt_dev, bool reset_min,
+                                  cudaStream_t s) {
+    const mc::StagePlan plan = mc::plan_for(c->scheme.time_stepper);
+    double* bufs[3] = {Q, c->buf_a, c->buf_b};
+    c->last_stage_in = bufs[plan.in[plan.n - 1]];
+    MC_CUDA(cudaEventRecord(c->ov_fork, s), "fork");
+    MC_CUDA(cudaStreamWaitEvent(c->ov_border, c->ov_fork, 0), "fork");
+    MC_CUDA(cudaStreamWaitEvent(c->ov_interior, c->ov_fork, 0), "fork");
+    MC_CUDA(cudaStreamWaitEvent(c->ov_comm, c->ov_fork, 0), "fork");
+    for (int st = 0; st < plan.n; ++st) {
+        StageParams p = base_params(c);
+        p.q_in = bufs[plan.in[st]];
+        p.q_old = Q;
+        p.q_out = bufs[plan.out[st]];
+        p.dt = dt;
+        p.dt_dev = dt_dev;
+        p.combo = plan.combo[st];
+        p.last = st == plan.n - 1;
+        // both pieces of the first stage reset the minimum the last stage forms
+        p.reset_min = (reset_min && st == 0) ? 1 : 0;
+        StageParams pb = p;
+        pb.row_split = c->ov_b0;
+        pb.row_skip = c->ov_b1 - c->ov_b0;
+        pb.tile_rows = c->ov_b0 + (c->ov_rows - c->ov_b1);
+        StageParams pi = p;
+        pi.row_split = 0;
+        pi.row_skip = c->ov_b0;
+        pi.tile_rows = c->ov_b1 - c->ov_b0;
+        if (st > 0) {
+            MC_CUDA(cudaStreamWaitEvent(c->ov_border, c->ov_interior_done[st - 1], 0), "wait");
+            MC_CUDA(cudaStreamWaitEvent(c->ov_border, c->ov_exch_done[st - 1], 0), "wait");
+            MC_CUDA(cudaStreamWaitEvent(c->ov_interior, c->ov_border_done[st - 1], 0), "wait");
+        }
+        mc_ctx::Timed t{nullptr, nullptr, 0, nullptr, nullptr};
+        if (c->profiling) {
+            t = mc_ctx::Timed{pooled_event(c), pooled_event(c), 0, pooled_event(c), pooled_event(c)};
+            cudaEventRecord(t.start, c->ov_border);
+        }
+        MC_CUDA(launch_stage_kernel(c, pb, 0, c->ov_border), "stage launch (border rows)");
+        if (c->profiling) {
+            cudaEventRecord(t.stop, c->ov_border);
+        }
+        MC_CUDA(cudaEventRecord(c->ov_border_done[st], c->ov_border), "event");
+        MC_CUDA(cudaStreamWaitEvent(c->ov_comm, c->ov_border_done[st], 0), "wait");
+        if (mc_status e = exchange_slab(c, p.q_out, c->ov_comm)) {
+            return e;
+        }
+        MC_CUDA(cudaEventRecord(c->ov_exch_done[st], c->ov_comm), "event");
+        if (c->profiling) {
+            cudaEventRecord(t.start2, c->ov_interior);
+        }
+        MC_CUDA(launch_stage_kernel(c, pi, 0, c->ov_interior), "stage launch (interior rows)");
+        if (c->profiling) {
+            cudaEventRecord(t.stop2, c->ov_interior);
+            c->timed.push_back(t);
+        }
+        MC_CUDA(cudaEventRecord(c->ov_interior_done[st], c->ov_interior), "event");
+    }
+    MC_CUDA(cudaStreamWaitEvent(s, c->ov_interior_done[plan.n - 1], 0), "join");
+    MC_CUDA(cudaStreamWaitEvent(s, c->ov_exch_done[plan.n - 1], 0), "join");
+    return MC_OK;
+}
+
 // The domain-wide reduction of the CFL minimum word: the slab
 // decomposition's all-reduce and the caller's hook, if any.
 mc_status reduce_cfl(mc_ctx* c, cudaStream_t s) {
@@ -302,6 +401,61 @@ double clamp_to_output(double dt, const mc_clock* k) {
         }
     }
     return dt;
+}
+
+// Streams, events and border tile rows of the overlapped slab step (2D).
+mc_status create_overlap(mc_ctx* c) {
+    const int ng = c->grid.ng, ny = c->ny;
+    const int rows = (ny + mc::kTile - 1) / mc::kTile;
+    // border rows: those whose tiles read ghost rows (first row y0 < H <= ng)
+    // or write layers that are sent (y0 < ng, or y1 > ny - ng)
+    int b0 = 0;
+    while (b0 < rows && b0 * mc::kTile < ng) {
+        ++b0;
+    }
+    int b1 = rows;
+    while (b1 > b0 && std::min(ny, b1 * mc::kTile) > ny - ng) {
+        --b1;
+    }
+    c->ov_b0 = b0;
+    c->ov_b1 = b1;
+    c->ov_rows = rows;
+    int least = 0, greatest = 0;
+    MC_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
+    MC_CUDA(cudaStreamCreateWithPriority(&c->ov_border, cudaStreamNonBlocking, greatest), "stream");
+    MC_CUDA(cudaStreamCreateWithPriority(&c->ov_comm, cudaStreamNonBlocking, greatest), "stream");
+    MC_CUDA(cudaStreamCreateWithPriority(&c->ov_interior, cudaStreamNonBlocking, least), "stream");
+    MC_CUDA(cudaEventCreateWithFlags(&c->ov_fork, cudaEventDisableTiming), "event");
+    for (int k = 0; k < 4; ++k) {
+        MC_CUDA(cudaEventCreateWithFlags(&c->ov_border_done[k], cudaEventDisableTiming), "event");
+        MC_CUDA(cudaEventCreateWithFlags(&c->ov_interior_done[k], cudaEventDisableTiming), "event");
+        MC_CUDA(cudaEventCreateWithFlags(&c->ov_exch_done[k], cudaEventDisableTiming), "event");
+    }
+    return MC_OK;
+}
+
+void destroy_overlap(mc_ctx* c) {
+    for (cudaStream_t* st : {&c->ov_border, &c->ov_interior, &c->ov_comm}) {
+        if (*st) {
+            cudaStreamSynchronize(*st);
+            cudaStreamDestroy(*st);
+            *st = nullptr;
+        }
+    }
+    for (cudaEvent_t* e : {&c->ov_fork}) {
+        if (*e) {
+            cudaEventDestroy(*e);
+            *e = nullptr;
+        }
+    }
+    for (int k = 0; k < 4; ++k) {
+        for (cudaEvent_t* e : {&c->ov_border_done[k], &c->ov_interior_done[k], &c->ov_exch_done[k]}) {
+            if (*e) {
+                cudaEventDestroy(*e);
+                *e = nullptr;
+            }
+        }
+    }
 }
 
 mc_status check_ctx(const mc_ctx* c) {
@@ -433,6 +587,7 @@ mc_status mc_destroy(mc_ctx* c) {
     if (!c) {
         return MC_OK;
     }
+    destroy_overlap(c);  // its streams drained before the communicator goes
     mc::slab_destroy(c->slab);
     cudaFree(c->buf_a);
     cudaFree(c->buf_b);
@@ -450,6 +605,10 @@ mc_status mc_destroy(mc_ctx* c) {
     for (auto& t : c->timed) {
         cudaEventDestroy(t.start);
         cudaEventDestroy(t.stop);
+        if (t.start2) {
+            cudaEventDestroy(t.start2);
+            cudaEventDestroy(t.stop2);
+        }
     }
     for (auto e : c->event_pool) {
         cudaEventDestroy(e);
@@ -517,6 +676,11 @@ mc_status mc_set_slab_decomposition(mc_ctx* c, const uint8_t* id, int32_t rank, 
     }
     c->slab = s;
     c->slab_faces = mc::slab_face_mask(s);
+    if (c->grid.num_dim == 2) {
+        if (mc_status st = create_overlap(c)) {
+            return st;
+        }
+    }
     // the kernels leave the exchanged faces' ghosts alone
     for (int f = f0; f < f0 + 2; ++f) {
         if ((c->slab_faces >> f) & 1) {
@@ -806,6 +970,14 @@ mc_status mc_get_status(mc_ctx* c, uint32_t* flags, void* stream) {
     return MC_OK;
 }
 
+mc_status mc_set_slab_overlap(mc_ctx* c, int32_t enable) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    c->slab_overlap = enable != 0;
+    return MC_OK;
+}
+
 mc_status mc_profile_stages(mc_ctx* c, int32_t enable) {
     if (mc_status st = check_ctx(c)) {
         return st;
@@ -813,6 +985,10 @@ mc_status mc_profile_stages(mc_ctx* c, int32_t enable) {
     for (auto& t : c->timed) {
         c->event_pool.push_back(t.start);
         c->event_pool.push_back(t.stop);
+        if (t.start2) {
+            c->event_pool.push_back(t.start2);
+            c->event_pool.push_back(t.stop2);
+        }
     }
     c->timed.clear();
     c->profiling = enable != 0;
@@ -835,6 +1011,14 @@ mc_status mc_stage_time(mc_ctx* c, int32_t kind, double* total_ms, int64_t* laun
         MC_CUDA(cudaEventSynchronize(t.stop), "event sync");
         float ms = 0.0f;
         MC_CUDA(cudaEventElapsedTime(&ms, t.start, t.stop), "event time");
+        if (t.start2) {
+            // the two pieces of an overlapped stage: first start to last stop
+            MC_CUDA(cudaEventSynchronize(t.stop2), "event sync");
+            float s2 = 0.0f, e2 = 0.0f;
+            MC_CUDA(cudaEventElapsedTime(&s2, t.start, t.start2), "event time");
+            MC_CUDA(cudaEventElapsedTime(&e2, t.start, t.stop2), "event time");
+            ms = std::max(ms, e2) - std::min(0.0f, s2);
+        }
         sum += ms;
         ++n;
     }

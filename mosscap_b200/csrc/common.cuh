@@ -64,9 +64,18 @@ struct StageParams {
     DeviceBlock* blk;
     int gravity;                      // nonzero: the gravity source term is registered
     double grav[3];                   // its acceleration (x, y, z)
+    // 2D launches over some of the tile rows (the slab exchange's overlap):
+    // tile row = blockIdx.y, plus row_skip from blockIdx.y = row_split on;
+    // tile_rows, if nonzero, is the launch's grid height. All zero: every
+    // tile row, one per blockIdx.y.
+    int row_split, row_skip, tile_rows;
 };
 
 constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;
+
+// Output cells per warp-wide row segment: the side of a 2D tile and the
+// length of a 1D segment or z column chunk.
+constexpr int kTile = 30;
 
 // Called at the top of every stage kernel: a stage that is not the last one
 // clears the CFL-minimum cell that the last stage will reduce into.

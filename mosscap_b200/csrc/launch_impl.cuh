@@ -71,7 +71,8 @@ cudaError_t launch_tiled(const StageParams& p, const CUtensorMap& map, cudaStrea
         if (e != cudaSuccess) {
             return e;
         }
-        const dim3 grid(cdiv(p.nx, kTile), cdiv(p.ny, kTile), NDIM == 3 ? p.nz : 1);
+        const int rows = (NDIM == 2 && p.tile_rows > 0) ? p.tile_rows : cdiv(p.ny, kTile);
+        const dim3 grid(cdiv(p.nx, kTile), rows, NDIM == 3 ? p.nz : 1);
         k<<<grid, dim3(tile_threads<NDIM, Real>()), sm, s>>>(p, map);
         return cudaGetLastError();
     }

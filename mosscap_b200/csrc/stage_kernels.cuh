@@ -33,7 +33,6 @@
 
 namespace mc {
 
-constexpr int kTile = 30;     // output cells per warp-wide row segment
 constexpr int kThreads = 256; // threads per CTA of the 1D and z-pass kernels (2D: tile_threads)
 constexpr int kWarps = kThreads / 32;
 // CTAs per SM of the 256-thread kernels: FP64 three (80 registers a
@@ -783,8 +782,9 @@ __global__ void __launch_bounds__(tile_threads<NDIM, T>(), tile_min_blocks<NDIM,
         // the tensor copy's destination: 128-byte aligned
         base += (128u - (smem_addr(smem_raw) & 127u)) & 127u;
     }
-    tile2d<NDIM, REC, LIM, RS, T, SRC, NT, TMA>(p, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<T*>(base),
-                                                dtmin, flags, &tmap, &mbar);
+    const int by = (int)blockIdx.y + ((int)blockIdx.y >= p.row_split ? p.row_skip : 0);
+    tile2d<NDIM, REC, LIM, RS, T, SRC, NT, TMA>(p, blockIdx.x, by, blockIdx.z, reinterpret_cast<T*>(base), dtmin,
+                                                flags, &tmap, &mbar);
     block_publish(dtmin, flags, NDIM != 3 && p.last != 0, p.blk, red_d, red_u);
 }
 

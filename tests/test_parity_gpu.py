@@ -407,3 +407,43 @@ def test_fp32_form_3d_tma_tiles_against_oracle(gpu_lib, oracle_port, nx, ny, nz)
     rel_l1 = np.abs(rho - rho_ref).sum() / np.abs(rho_ref).sum()
     assert rel_l1 < 1e-6, rel_l1
     assert sim.status() == 0
+
+
+@pytest.mark.parametrize("ny,st,rec,rs,gravity", [(121, "rk2", "ppm", "hll", None),
+                                                  (97, "ssprk3", "weno5z", "hllc", (0.3, -1.0, 0.0)),
+                                                  (150, "ssprk4", "muscl", "rusanov", None)])
+def test_slab_overlap_single_rank(gpu_lib, oracle_port, ny, st, rec, rs, gravity):
+    """A 2D slab whose exchange runs beside the interior tile rows
+    (mc_set_slab_overlap, on by default; one rank exchanging with itself
+    through the library's NCCL path): bit-identical to the oracle and to the
+    same slab with the overlap off, in the device- and host-driven loops,
+    with stage timing on (one timed interval per stage). ny = 121 leaves one
+    row in the last tile row, fewer than ng, so two tile rows at that end
+    write layers that are sent."""
+    from mosscap_b200 import capi
+    from mosscap_b200.distributed import SlabSim
+    nx, steps = 70, 10
+    q = P.random_state(2, nx, ny, ng=3, seed=ny)
+    p = P.Problem("slab_overlap", 2, nx, ny, ng=3, dx=1.0 / ny,
+                  bc=("wall", "zerograd", "periodic", "periodic", "zerograd", "zerograd"),
+                  reconstruction=rec, slope_limiter="vanleer", riemann_solver=rs, time_stepper=st, gamma=1.4,
+                  max_cfl=0.4, max_time=1e30, output_delta=1e30, gravity=gravity, Q=q)
+    o = _oracle(oracle_port, p)
+    ref_dts = o.run(steps)
+    ref = o.get_Q()
+    nst = {"rk2": 2, "ssprk3": 3, "ssprk4": 4}[st]
+    for overlap in (1, 0):
+        for loop in ("device", "host"):
+            s = SlabSim(p, rank=0, world=1, transport="library")
+            capi.check(s.sim.lib.mc_set_slab_overlap(s.sim.ctx, overlap), "mc_set_slab_overlap")
+            s.fill_bcs()
+            s.sim.profile_stages(True)
+            dts = s.advance(steps) if loop == "device" else [s.step() for _ in range(steps)]
+            ms, n = s.sim.stage_time(0)
+            s.sim.profile_stages(False)
+            what = f"overlap={overlap} {loop}"
+            _assert_same(np.array(dts), ref_dts, f"dt ({what})")
+            _assert_same(s.sim.get_Q(), ref, f"state ({what})")
+            assert n == steps * nst and ms > 0.0, (what, n, ms)
+            assert s.sim.status() == 0
+            s.sim.close()
