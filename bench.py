@@ -356,9 +356,8 @@ def run_ours(args):
         host = torch.empty(sim.Q.shape, dtype=torch.float64, pin_memory=True)
         host.copy_(sim.Q)
         qbytes = host.numel() * 8
-        barrier()
-        t0 = time.perf_counter()
-        for _ in range(K):
+
+        def serial_step():
             sim.Q.copy_(host, non_blocking=True)
             if slab is not None:
                 slab.step()                # global dt read back on the host, then the step
@@ -367,12 +366,32 @@ def run_ours(args):
                 sim.time_step(dt)
             host.copy_(sim.Q, non_blocking=True)
             torch.cuda.synchronize(dev)
-        barrier()
-        secs = max_over_ranks(time.perf_counter() - t0)
+
+        def timed(step):
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(K):
+                step()
+            barrier()
+            return max_over_ranks(time.perf_counter() - t0)
+
+        secs_serial = timed(serial_step)
+        if slab is None:
+            # mc_step_host: the same copies and step in one call, the copies
+            # overlapping the step
+            secs = timed(lambda: sim.step_host(host))
+            how = ("per step: mc_step_host on a pinned-host state (state -> device band by band with stage 0's "
+                   "fluxes computed behind it, dt on the device, the step, the last stage band by band with each "
+                   "band's rows copied back behind it), dt read back, synchronize")
+        else:
+            secs = secs_serial
+            how = ("per step: pinned-host state -> device, global dt (mc_compute_dt with the slab all-reduce, read "
+                   "back), mc_time_step, state -> pinned host, synchronize")
         e2e = {"value": world * cells * K / secs, "unit": UNIT, "h2d_bytes_per_step": qbytes,
-               "d2h_bytes_per_step": qbytes + 8,
-               "how": "per step: pinned-host state -> device, mc_compute_dt (dt read back), mc_time_step, "
-                      "state -> pinned host, synchronize"}
+               "d2h_bytes_per_step": qbytes + 8, "how": how,
+               "serial_calls_value": world * cells * K / secs_serial,
+               "serial_calls_how": "per step: pinned-host state -> device, mc_compute_dt (dt read back), "
+                                   "mc_time_step, state -> pinned host, synchronize"}
 
     # ---- the other forms, measured in this run (rank 0, N = 1) ------------
     extras = None

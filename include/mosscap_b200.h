@@ -265,6 +265,23 @@ mc_status mc_compute_dt(mc_ctx* ctx, const double* Q, const mc_clock* clock, dou
  * last stage and can be read with mc_last_cfl_min. */
 mc_status mc_time_step(mc_ctx* ctx, double* Q, double dt, void* stream);
 
+/* compute_dt + time_step (source/main.cpp:55-56) on a state that lives in
+ * host memory, for a caller that keeps it there between steps (a CPU build
+ * of Mosscap handing its step to the GPU): Q_host is copied into Q (a device
+ * array of the same layout, the caller's), dt is formed as mc_compute_dt
+ * forms it under *clock (no output clamp when clock is NULL), one step is
+ * taken, the result is copied back into Q_host and *dt_out = dt. Results are
+ * those of the copies plus mc_compute_dt plus mc_time_step. In 2D (ideal
+ * EOS, no user or CFL hook, no slab exchange, more than 30 interior rows)
+ * the copies overlap the step: stage 0's fluxes are computed band of rows by
+ * band as the state arrives and dt is applied once all of it is in; the last
+ * stage runs band by band, each band copied back behind it. Q_host should be
+ * pinned (cudaHostAlloc) for the copies to overlap. *clock is not advanced.
+ * A dt that is not positive and finite fails with MC_ERR_INVALID_ARGUMENT
+ * and no step. Waits for the stream. */
+mc_status mc_step_host(mc_ctx* ctx, double* Q_host, double* Q, const mc_clock* clock, double* dt_out,
+                       void* stream);
+
 /* The main loop of source/main.cpp:54-72 on the device: up to max_steps of
  * { dt = compute_dt; time_step(dt); time += dt } stopping after the step
  * that reaches max_time or an output time (prev_output_time + output_delta),

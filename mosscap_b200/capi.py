@@ -127,6 +127,8 @@ def load() -> ctypes.CDLL:
     lib.mc_compute_dt.restype = i32
     lib.mc_time_step.argtypes = [vp, vp, d, vp]
     lib.mc_time_step.restype = i32
+    lib.mc_step_host.argtypes = [vp, vp, vp, P(McClock), P(d), vp]
+    lib.mc_step_host.restype = i32
     lib.mc_advance.argtypes = [vp, vp, P(McClock), i64, P(i64), P(d), vp]
     lib.mc_advance.restype = i32
     lib.mc_last_cfl_min.argtypes = [vp, P(d), vp]

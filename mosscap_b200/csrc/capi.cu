@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <new>
 #include <string>
 #include <vector>
@@ -50,6 +51,10 @@ struct mc_ctx {
     cudaStream_t ov_border = nullptr, ov_interior = nullptr, ov_comm = nullptr;
     cudaEvent_t ov_fork = nullptr;
     cudaEvent_t ov_border_done[4] = {}, ov_interior_done[4] = {}, ov_exch_done[4] = {};
+    // mc_step_host: copy streams and events of its pipeline (created on first use)
+    cudaStream_t hs_in = nullptr, hs_out = nullptr;
+    cudaEvent_t hs_fork = nullptr, hs_join = nullptr;
+    cudaEvent_t hs_ev_in[8] = {}, hs_ev_out[8] = {};
     int gravity = 0;              // mc_set_gravity
     double grav[3] = {0.0, 0.0, 0.0};
     // non-ideal EOS (mc_set_eos)
@@ -374,6 +379,177 @@ mc_status enqueue_step_overlapped(mc_ctx* c, double* Q, double dt, const double*
     return MC_OK;
 }
 
+// ---- mc_step_host ------------------------------------------------------------
+
+constexpr int kHostBands = 8;  // bands of tile rows of the pipelined host step
+
+// Whether mc_step_host overlaps its copies with the step (2D, ideal EOS, no
+// hooks or slab exchange, at least two tile rows).
+bool host_pipelined(const mc_ctx* c) {
+    return c->grid.num_dim == 2 && c->eos_type == mc::kEosIdeal && !c->user_bc && !c->slab && !c->cfl_hook &&
+           c->ny > mc::kTile;
+}
+
+mc_status create_host_streams(mc_ctx* c) {
+    if (c->hs_in) {
+        return MC_OK;
+    }
+    MC_CUDA(cudaStreamCreateWithFlags(&c->hs_in, cudaStreamNonBlocking), "stream");
+    MC_CUDA(cudaStreamCreateWithFlags(&c->hs_out, cudaStreamNonBlocking), "stream");
+    MC_CUDA(cudaEventCreateWithFlags(&c->hs_fork, cudaEventDisableTiming), "event");
+    MC_CUDA(cudaEventCreateWithFlags(&c->hs_join, cudaEventDisableTiming), "event");
+    for (int b = 0; b < kHostBands; ++b) {
+        MC_CUDA(cudaEventCreateWithFlags(&c->hs_ev_in[b], cudaEventDisableTiming), "event");
+        MC_CUDA(cudaEventCreateWithFlags(&c->hs_ev_out[b], cudaEventDisableTiming), "event");
+    }
+    return MC_OK;
+}
+
+void destroy_host_streams(mc_ctx* c) {
+    for (cudaStream_t* st : {&c->hs_in, &c->hs_out}) {
+        if (*st) {
+            cudaStreamSynchronize(*st);
+            cudaStreamDestroy(*st);
+            *st = nullptr;
+        }
+    }
+    for (cudaEvent_t* e : {&c->hs_fork, &c->hs_join}) {
+        if (*e) {
+            cudaEventDestroy(*e);
+            *e = nullptr;
+        }
+    }
+    for (int b = 0; b < kHostBands; ++b) {
+        for (cudaEvent_t* e : {&c->hs_ev_in[b], &c->hs_ev_out[b]}) {
+            if (*e) {
+                cudaEventDestroy(*e);
+                *e = nullptr;
+            }
+        }
+    }
+}
+
+// The pipelined host step (2D). The grid's tile rows split into bands.
+//  1. The state arrives band by band (rows of all variables, one 2D copy per
+//     band) on hs_in; stage 0's tiles of a band run as soon as the rows they
+//     read have arrived, writing only their x+y divergence (into buf_b,
+//     which no stage before the second reads).
+//  2. Once the whole state is in: the CFL minimum and dt (the device clock,
+//     the output clamp of compute_dt), then the rest of stage 0 per cell
+//     (finish2d_kernel: the same operations the tiles would have done).
+//  3. The middle stages whole; the last stage band by band, each band's
+//     interior rows copied back on hs_out as soon as it is done (no later
+//     band writes them), the ghost rows after the last band.
+// Result and dt are those of compute_dt + time_step.
+mc_status step_host_pipelined(mc_ctx* c, double* Qh, double* Q, const mc_clock* clk, double* dt_out,
+                              cudaStream_t s) {
+    if (mc_status st = create_host_streams(c)) {
+        return st;
+    }
+    const mc::StagePlan plan = mc::plan_for(c->scheme.time_stepper);
+    double* bufs[3] = {Q, c->buf_a, c->buf_b};
+    const int ng = c->grid.ng, ny = c->ny;
+    const long long xc = c->grid.xc, yc = c->grid.yc;
+    const int rows = (ny + mc::kTile - 1) / mc::kTile;
+    const int nb = std::min(kHostBands, rows);
+    int t[kHostBands + 1];
+    for (int b = 0; b <= nb; ++b) {
+        t[b] = (int)((long long)b * rows / nb);
+    }
+    // padded-row boundaries of the input bands: the first and last also
+    // carry the ghost rows
+    auto in_row = [&](int b) -> long long { return b == 0 ? 0 : (b == nb ? yc : ng + (long long)t[b] * mc::kTile); };
+    const size_t pitch = sizeof(double) * (size_t)c->plane;
+    const size_t row_bytes = sizeof(double) * (size_t)xc;
+    const int nvar = c->nvar;
+    MC_CUDA(cudaEventRecord(c->hs_fork, s), "fork");
+    MC_CUDA(cudaStreamWaitEvent(c->hs_in, c->hs_fork, 0), "fork");
+    MC_CUDA(cudaStreamWaitEvent(c->hs_out, c->hs_fork, 0), "fork");
+    for (int b = 0; b < nb; ++b) {
+        const long long r0 = in_row(b), r1 = in_row(b + 1);
+        MC_CUDA(cudaMemcpy2DAsync(Q + r0 * xc, pitch, Qh + r0 * xc, pitch, (size_t)(r1 - r0) * row_bytes, nvar,
+                                  cudaMemcpyHostToDevice, c->hs_in),
+                "state in");
+        MC_CUDA(cudaEventRecord(c->hs_ev_in[b], c->hs_in), "event");
+    }
+    const double inf = std::numeric_limits<double>::infinity();
+    MC_CUDA(mc::launch_clock_init(c->blk, clk ? clk->time : 0.0, clk ? clk->max_time : inf,
+                                  clk ? clk->prev_output_time : 0.0, clk ? clk->output_delta : inf,
+                                  c->scheme.max_cfl, s),
+            "clock init");
+    // 1. stage 0's divergence, band by band
+    StageParams d = base_params(c);
+    d.q_in = Q;
+    d.q_old = Q;
+    d.q_out = bufs[plan.out[0]];
+    d.dqxy = c->buf_b;
+    d.combo = plan.combo[0];
+    for (int b = 0; b < nb; ++b) {
+        // the band's tiles read H rows of the next band
+        MC_CUDA(cudaStreamWaitEvent(s, c->hs_ev_in[std::min(b + 1, nb - 1)], 0), "wait");
+        StageParams pb = d;
+        pb.row_skip = t[b];
+        pb.tile_rows = t[b + 1] - t[b];
+        MC_CUDA(launch_stage_kernel(c, pb, 0, s), "stage 0 divergence");
+    }
+    // 2. dt, then the rest of stage 0
+    StageParams g = base_params(c);
+    g.q_in = Q;
+    MC_CUDA(mc::launch_cfl_min(g, 2, s), "cfl_min");
+    MC_CUDA(mc::launch_clock_advance(c->blk, nullptr, 1, s), "clock");
+    c->launches += 3;
+    const double* dt_dev = &c->blk->dt;
+    StageParams f = d;
+    f.dt_dev = dt_dev;
+    MC_CUDA(launch_stage_kernel(c, f, 2, s), "stage 0 finish");
+    // 3. the other stages; the last one band by band behind the copies
+    for (int st = 1; st < plan.n; ++st) {
+        StageParams p = base_params(c);
+        p.q_in = bufs[plan.in[st]];
+        p.q_old = Q;
+        p.q_out = bufs[plan.out[st]];
+        p.dt_dev = dt_dev;
+        p.combo = plan.combo[st];
+        p.last = st == plan.n - 1;
+        if (!p.last) {
+            MC_CUDA(launch_stage_kernel(c, p, 0, s), "stage launch");
+            continue;
+        }
+        for (int b = 0; b < nb; ++b) {
+            StageParams pb = p;
+            pb.row_skip = t[b];
+            pb.tile_rows = t[b + 1] - t[b];
+            MC_CUDA(launch_stage_kernel(c, pb, 0, s), "last stage");
+            MC_CUDA(cudaEventRecord(c->hs_ev_out[b], s), "event");
+            MC_CUDA(cudaStreamWaitEvent(c->hs_out, c->hs_ev_out[b], 0), "wait");
+            const long long r0 = ng + (long long)t[b] * mc::kTile;
+            const long long r1 = ng + std::min((long long)ny, (long long)t[b + 1] * mc::kTile);
+            MC_CUDA(cudaMemcpy2DAsync(Qh + r0 * xc, pitch, Q + r0 * xc, pitch, (size_t)(r1 - r0) * row_bytes, nvar,
+                                      cudaMemcpyDeviceToHost, c->hs_out),
+                    "state out");
+        }
+    }
+    c->last_stage_in = bufs[plan.in[plan.n - 1]];
+    // the ghost rows (the end bands' scatter writes them) and the clock
+    MC_CUDA(cudaMemcpy2DAsync(Qh, pitch, Q, pitch, (size_t)ng * row_bytes, nvar, cudaMemcpyDeviceToHost, c->hs_out),
+            "ghost rows out");
+    MC_CUDA(cudaMemcpy2DAsync(Qh + (ng + (long long)ny) * xc, pitch, Q + (ng + (long long)ny) * xc, pitch,
+                              (size_t)ng * row_bytes, nvar, cudaMemcpyDeviceToHost, c->hs_out),
+            "ghost rows out");
+    MC_CUDA(cudaMemcpyAsync(c->blk_host, c->blk, sizeof(mc::DeviceBlock), cudaMemcpyDeviceToHost, c->hs_out),
+            "read-back");
+    MC_CUDA(cudaEventRecord(c->hs_join, c->hs_out), "join");
+    MC_CUDA(cudaStreamWaitEvent(s, c->hs_join, 0), "join");
+    MC_CUDA(cudaStreamSynchronize(s), "sync");
+    c->min_from_clock = false;
+    const mc::DeviceBlock& k = *c->blk_host;
+    *dt_out = k.dt;
+    if (k.done) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "dt must be positive and finite (the step was not taken)");
+    }
+    return MC_OK;
+}
+
 // The domain-wide reduction of the CFL minimum word: the slab
 // decomposition's all-reduce and the caller's hook, if any.
 mc_status reduce_cfl(mc_ctx* c, cudaStream_t s) {
@@ -588,6 +764,7 @@ mc_status mc_destroy(mc_ctx* c) {
         return MC_OK;
     }
     destroy_overlap(c);  // its streams drained before the communicator goes
+    destroy_host_streams(c);
     mc::slab_destroy(c->slab);
     cudaFree(c->buf_a);
     cudaFree(c->buf_b);
@@ -966,6 +1143,34 @@ mc_status mc_get_status(mc_ctx* c, uint32_t* flags, void* stream) {
     *flags = c->blk_host->status;
     const unsigned zero = 0;
     MC_CUDA(cudaMemcpyAsync(&c->blk->status, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, s), "clear");
+    MC_CUDA(cudaStreamSynchronize(s), "sync");
+    return MC_OK;
+}
+
+mc_status mc_step_host(mc_ctx* c, double* Q_host, double* Q, const mc_clock* clock, double* dt_out, void* stream) {
+    if (mc_status st = check_ctx(c)) {
+        return st;
+    }
+    if (!Q_host || !Q || !dt_out) {
+        return fail(MC_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    if (mc_status st = check_user_bc(c)) {
+        return st;
+    }
+    const cudaStream_t s = (cudaStream_t)stream;
+    if (host_pipelined(c)) {
+        return step_host_pipelined(c, Q_host, Q, clock, dt_out, s);
+    }
+    MC_CUDA(cudaMemcpyAsync(Q, Q_host, c->state_bytes, cudaMemcpyHostToDevice, s), "state in");
+    double dt = 0.0;
+    if (mc_status st = mc_compute_dt(c, Q, clock, &dt, stream)) {
+        return st;
+    }
+    *dt_out = dt;
+    if (mc_status st = mc_time_step(c, Q, dt, stream)) {
+        return st;
+    }
+    MC_CUDA(cudaMemcpyAsync(Q_host, Q, c->state_bytes, cudaMemcpyDeviceToHost, s), "state out");
     MC_CUDA(cudaStreamSynchronize(s), "sync");
     return MC_OK;
 }

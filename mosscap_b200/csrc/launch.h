@@ -28,7 +28,9 @@ inline StagePlan plan_for(int stepper) {
 }
 
 // One stage of an SSPRK step. pass selects, in 3D, the x-y plane pass (0)
-// or the z pass that finishes the stage (1); it is ignored in 1D and 2D.
+// or the z pass that finishes the stage (1); in 2D, the stage (0) or the
+// finishing of a stage whose tiles wrote only their divergence into
+// p.dqxy (2); it is ignored in 1D.
 cudaError_t launch_stage_d1_fp64(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
 cudaError_t launch_stage_d2_fp64(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
 cudaError_t launch_stage_d3_fp64(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);

@@ -159,7 +159,18 @@ cudaError_t by_solver(const StageParams& p, int rs, int pass, cudaStream_t s) {
 
 // Dispatch on (reconstruction, limiter, solver). The limiter only matters for
 // MUSCL and PPM; FOG and WENO5-Z are limiter-agnostic (Reconstruct.hpp:33-44).
+// In 2D, pass 2 is the finishing of a stage whose tiles wrote only their
+// divergence (finish2d_kernel), whatever the scheme.
 cudaError_t MC_LAUNCH_NAME(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s) {
+#if MC_DIM == 2
+    if (pass == 2) {
+        const long long cells = (long long)p.nx * p.ny;
+        const long long want = (cells + kThreads - 1) / kThreads;
+        const int blocks = (int)(want < 148LL * 8 ? want : 148LL * 8);
+        finish2d_kernel<Real, MC_SRC><<<blocks, kThreads, 0, s>>>(p);
+        return cudaGetLastError();
+    }
+#endif
     switch (rec) {
         case kFog:
             return by_solver<kFog, kMonotonizedCentral>(p, rs, pass, s);

@@ -675,9 +675,12 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
             const T* dfy = DY + line * PY + c;
             const int i = p.ng + x0 + c;
             const int j = p.ng + y0 + line;
-            if constexpr (NDIM == 3) {
+            // 3D, and a 2D stage given a divergence buffer (finished later by
+            // finish2d_kernel once dt is known): the x+y divergence only
+            if (NDIM == 3 || p.dqxy) {
                 const long long cells = (long long)p.nx * p.ny * p.nz;
-                const long long o = ((long long)(k - p.ng) * p.ny + (j - p.ng)) * p.nx + (i - p.ng);
+                const long long kz = NDIM == 3 ? k - p.ng : 0;
+                const long long o = (kz * p.ny + (j - p.ng)) * p.nx + (i - p.ng);
 #pragma unroll
                 for (int v = 0; v < nh; ++v) {
                     double qu = 0.0;
@@ -732,6 +735,67 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
         }
         __syncthreads();
     }
+}
+
+// The rest of a 2D stage whose tiles wrote only their x+y divergence
+// (p.dqxy, [var][y][x] over the interior cells): per interior cell, x
+// fastest, q_update = that divergence times dt / dx, the source term, the
+// stage combination, the store and the ghost scatter, as the tile's own
+// finishing does with the same operations in the same order. Lets a step
+// compute stage 0's fluxes before dt is known.
+template <class T, bool SRC>
+__global__ void __launch_bounds__(kThreads) finish2d_kernel(StageParams p) {
+    if (p.dt_dev && p.blk->done) {
+        return;
+    }
+    constexpr int NDIM = 2;
+    constexpr int nh = 4;
+    __shared__ double red_d[kWarps];
+    __shared__ unsigned red_u[kWarps];
+    double dtmin = __longlong_as_double(0x7ff0000000000000ll);
+    unsigned flags = 0;
+    const double dt = stage_dt(p);
+    const double dtdx = dt / p.dx;
+    const bool old = combo_reads_old(p.combo);
+    const int ntr = p.ntracer;
+    const long long cells = (long long)p.nx * p.ny;
+    const long long vs = (long long)p.zc * p.yc * p.xc;
+    for (long long o = blockIdx.x * (long long)kThreads + threadIdx.x; o < cells;
+         o += (long long)gridDim.x * kThreads) {
+        const int y = (int)(o / p.nx);
+        const int x = (int)(o - (long long)y * p.nx);
+        const int i = p.ng + x, j = p.ng + y;
+        const long long id0 = qidx(p, 0, 0, j, i);
+        double qo[nh], qi[nh], qu[nh], sdt[nh];
+#pragma unroll
+        for (int v = 0; v < nh; ++v) {
+            qi[v] = p.q_in[id0 + v * vs];
+            qo[v] = old ? p.q_old[id0 + v * vs] : 0.0;
+        }
+        source_dt_of<NDIM, SRC>(p, qi, dt, sdt);
+#pragma unroll
+        for (int v = 0; v < nh; ++v) {
+            qu[v] = p.dqxy[v * cells + o];
+            qu[v] *= dtdx;
+        }
+        double qn[kMaxVars];
+#pragma unroll
+        for (int v = nh; v < kMaxVars; ++v) {
+            qn[v] = 0.0;
+        }
+        combine_all<nh>(p.combo, qo, qi, qu, sdt, qn);
+#pragma unroll
+        for (int t = 0; t < kMaxVars - nh; ++t) {
+            if (t < ntr) {
+                double qt = p.dqxy[(nh + t) * cells + o];
+                qt *= dtdx;
+                const long long id = id0 + (nh + t) * vs;
+                qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qt, 0.0);
+            }
+        }
+        dtmin = smin(write_cell<NDIM, T>(p, i, j, 0, qn, p.last != 0, &flags), dtmin);
+    }
+    block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
 }
 
 // Threads per CTA of the tiled stage kernel and CTAs per SM it is compiled

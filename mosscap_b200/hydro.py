@@ -138,6 +138,23 @@ class HydroSim:
         self.time += dt
         self.current_step += 1
 
+    def step_host(self, q_host: torch.Tensor, clamp: bool = True) -> float:
+        """compute_dt + time_step on a host-resident state (mc_step_host):
+        q_host (float64 CPU tensor of Q's shape, pinned for the copies to
+        overlap the step) goes to the device copy Q, one step is taken there
+        and the result returns to q_host. Advances the clock like time_step;
+        returns dt."""
+        assert q_host.device.type == "cpu" and q_host.dtype == torch.float64 and q_host.is_contiguous()
+        assert tuple(q_host.shape) == tuple(self.Q.shape)
+        dt = ctypes.c_double()
+        clk = self._clock()
+        capi.check(self.lib.mc_step_host(self.ctx, ctypes.c_void_p(q_host.data_ptr()), self._qptr(),
+                                         ctypes.byref(clk) if clamp else None, ctypes.byref(dt), self._stream()),
+                   "mc_step_host")
+        self.time += dt.value
+        self.current_step += 1
+        return dt.value
+
     def last_cfl_min(self) -> float:
         v = ctypes.c_double()
         capi.check(self.lib.mc_last_cfl_min(self.ctx, ctypes.byref(v), self._stream()), "mc_last_cfl_min")
