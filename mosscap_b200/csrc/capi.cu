@@ -167,6 +167,15 @@ cudaError_t launch_stage_kernel(mc_ctx* c, const StageParams& p, int pass, cudaS
     const bool f32 = c->scheme.precision == MC_PRECISION_FP32_COMPENSATED;
     const int r = c->scheme.reconstruction, l = c->scheme.slope_limiter, rs = c->scheme.riemann_solver;
     c->launches += 1;
+    if (nd == 2 && pass == 0 && p.dqxy) {
+        // the deferred form (mc_step_host)
+        if (p.gravity) {
+            return f32 ? mc::launch_stage_d2_fp32_src_defer(p, r, l, rs, pass, s)
+                       : mc::launch_stage_d2_fp64_src_defer(p, r, l, rs, pass, s);
+        }
+        return f32 ? mc::launch_stage_d2_fp32_defer(p, r, l, rs, pass, s)
+                   : mc::launch_stage_d2_fp64_defer(p, r, l, rs, pass, s);
+    }
     if (p.gravity) {
         if (nd == 1) {
             return f32 ? mc::launch_stage_d1_fp32_src(p, r, l, rs, pass, s)

@@ -29,8 +29,8 @@ inline StagePlan plan_for(int stepper) {
 
 // One stage of an SSPRK step. pass selects, in 3D, the x-y plane pass (0)
 // or the z pass that finishes the stage (1); in 2D, the stage (0) or the
-// finishing of a stage whose tiles wrote only their divergence into
-// p.dqxy (2); it is ignored in 1D.
+// finishing (2) of a stage whose deferred-form tiles wrote only their
+// divergence into p.dqxy; it is ignored in 1D.
 cudaError_t launch_stage_d1_fp64(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
 cudaError_t launch_stage_d2_fp64(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
 cudaError_t launch_stage_d3_fp64(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
@@ -44,6 +44,12 @@ cudaError_t launch_stage_d3_fp64_src(const StageParams& p, int rec, int lim, int
 cudaError_t launch_stage_d1_fp32_src(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
 cudaError_t launch_stage_d2_fp32_src(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
 cudaError_t launch_stage_d3_fp32_src(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+// 2D, the deferred form of the stage (pass 0 only): the tiles write their x+y
+// divergence into p.dqxy, and pass 2 of the regular launcher finishes it.
+cudaError_t launch_stage_d2_fp64_defer(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d2_fp32_defer(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d2_fp64_src_defer(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
+cudaError_t launch_stage_d2_fp32_src_defer(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s);
 
 // Ghost fill of Q from its interior (every built-in boundary kind).
 cudaError_t launch_fill_bcs(const StageParams& p, int ndim, cudaStream_t s);

@@ -25,6 +25,12 @@
 #ifndef MC_SRC
 #define MC_SRC 0
 #endif
+// MC_DEFER 1 (2D): the deferred form of the stage kernel, whose tiles write
+// only their x+y divergence (for mc_step_host); in units of their own, so
+// the regular kernels compile as before.
+#ifndef MC_DEFER
+#define MC_DEFER 0
+#endif
 
 namespace mc {
 namespace {
@@ -65,7 +71,7 @@ cudaError_t launch_tiled(const StageParams& p, const CUtensorMap& map, cudaStrea
     if constexpr (TMA && !tma_capable<NDIM, REC, Real>(2 + NDIM)) {
         return cudaErrorNotSupported;  // never taken: use_tma refused it
     } else {
-        auto k = stage2d_kernel<NDIM, REC, LIM, RS, Real, SRC, TMA>;
+        auto k = stage2d_kernel<NDIM, REC, LIM, RS, Real, SRC, TMA, (NDIM == 2 && MC_DEFER != 0)>;
         const size_t sm = TMA ? smem_bytes_tma<NDIM, REC, Real>(p.nvar) : smem_bytes<NDIM, REC, Real>(p.nvar);
         cudaError_t e = allow_smem(k, sm);
         if (e != cudaSuccess) {
@@ -162,7 +168,7 @@ cudaError_t by_solver(const StageParams& p, int rs, int pass, cudaStream_t s) {
 // In 2D, pass 2 is the finishing of a stage whose tiles wrote only their
 // divergence (finish2d_kernel), whatever the scheme.
 cudaError_t MC_LAUNCH_NAME(const StageParams& p, int rec, int lim, int rs, int pass, cudaStream_t s) {
-#if MC_DIM == 2
+#if MC_DIM == 2 && !MC_DEFER
     if (pass == 2) {
         const long long cells = (long long)p.nx * p.ny;
         const long long want = (cells + kThreads - 1) / kThreads;

@@ -539,7 +539,8 @@ __global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
 // describes; the conserved tile arrives by one tensor copy (tmap, completed
 // on mbar) instead of per-thread loads. Without TMA, smem holds W and then
 // the y divergences (smem_bytes).
-template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false, int NT = kThreads, bool TMA = false>
+template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false, int NT = kThreads, bool TMA = false,
+          bool DEFER = false>
 __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int bz, T* smem, double& dtmin,
                                        unsigned& flags, const CUtensorMap* tmap = nullptr, uint64_t* mbar = nullptr) {
     constexpr int nh = 2 + NDIM;
@@ -675,9 +676,9 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
             const T* dfy = DY + line * PY + c;
             const int i = p.ng + x0 + c;
             const int j = p.ng + y0 + line;
-            // 3D, and a 2D stage given a divergence buffer (finished later by
+            // 3D, and the deferred form of a 2D stage (finished later by
             // finish2d_kernel once dt is known): the x+y divergence only
-            if (NDIM == 3 || p.dqxy) {
+            if constexpr (NDIM == 3 || DEFER) {
                 const long long cells = (long long)p.nx * p.ny * p.nz;
                 const long long kz = NDIM == 3 ? k - p.ng : 0;
                 const long long o = (kz * p.ny + (j - p.ng)) * p.nx + (i - p.ng);
@@ -827,7 +828,8 @@ __host__ __device__ constexpr bool tma_capable(int nvar) {
            (size_t)tile_min_blocks<NDIM, T>() * (smem_bytes_tma<NDIM, REC, T>(nvar) + 1024 + 256) <= 233472;
 }
 
-template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false, bool TMA = false>
+// DEFER (2D): the tiles write only their x+y divergence into p.dqxy.
+template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false, bool TMA = false, bool DEFER = false>
 __global__ void __launch_bounds__(tile_threads<NDIM, T>(), tile_min_blocks<NDIM, T>())
     stage2d_kernel(StageParams p, const __grid_constant__ CUtensorMap tmap) {
     if (p.dt_dev && p.blk->done) {
@@ -847,8 +849,8 @@ __global__ void __launch_bounds__(tile_threads<NDIM, T>(), tile_min_blocks<NDIM,
         base += (128u - (smem_addr(smem_raw) & 127u)) & 127u;
     }
     const int by = (int)blockIdx.y + ((int)blockIdx.y >= p.row_split ? p.row_skip : 0);
-    tile2d<NDIM, REC, LIM, RS, T, SRC, NT, TMA>(p, blockIdx.x, by, blockIdx.z, reinterpret_cast<T*>(base), dtmin,
-                                                flags, &tmap, &mbar);
+    tile2d<NDIM, REC, LIM, RS, T, SRC, NT, TMA, DEFER>(p, blockIdx.x, by, blockIdx.z, reinterpret_cast<T*>(base),
+                                                       dtmin, flags, &tmap, &mbar);
     block_publish(dtmin, flags, NDIM != 3 && p.last != 0, p.blk, red_d, red_u);
 }
 
