@@ -39,6 +39,9 @@ struct mc_batch {
     int ntasks1d = 0;
     int tasks_segs = 0;                  // segments per task the 1D list was built with
     int* d_counters = nullptr;           // one work counter per stage and part (kCounters)
+    int* d_finished = nullptr;           // per stage and problem: work items finished (ghost fill)
+    int* d_items_of = nullptr;           // per problem: its work items in a stage
+    std::vector<int> tiles_of;           // per problem: its 2D tiles (0 for 1D problems)
     double* buf_a = nullptr;
     double* buf_b = nullptr;
     cudaStream_t stream = nullptr;
@@ -144,8 +147,9 @@ __global__ void __launch_bounds__(256) batch_cfl_kernel(const StageParams* probs
 
 // One thread per problem: close its step (unless first) and pick its next
 // dt; outputs only advance the problem's clock. Thread 0 also resets the
-// work counters of the next step's stage launches.
-__global__ void batch_clock_kernel(DeviceBlock* blocks, int n, int first, int* counters) {
+// work counters of the next step's stage launches, and each thread its
+// problem's finished-item counts.
+__global__ void batch_clock_kernel(DeviceBlock* blocks, int n, int first, int* counters, int* finished) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         for (int c = 0; c < kCounters; ++c) {
@@ -153,6 +157,9 @@ __global__ void batch_clock_kernel(DeviceBlock* blocks, int n, int first, int* c
         }
     }
     if (i < n) {
+        for (int st = 0; st < 4; ++st) {
+            finished[st * n + i] = 0;
+        }
         mc::advance_clock(&blocks[i], nullptr, first != 0, false);
     }
 }
@@ -214,12 +221,16 @@ mc_status build_tasks(mc_batch* b, int segs) {
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return b->cells[a] > b->cells[c]; });
     std::vector<BatchTask1d> tasks;
+    std::vector<int> items_of(b->tiles_of);
     for (int i : order) {
         const int nseg = cdiv(b->params[i].nx, mc::kTile);
         for (int s0 = 0; s0 < nseg; s0 += segs) {
             tasks.push_back({i, s0, std::min(segs, nseg - s0), 0});
+            items_of[i] += 1;
         }
     }
+    MCB_CUDA(cudaMemcpy(b->d_items_of, items_of.data(), sizeof(int) * items_of.size(), cudaMemcpyHostToDevice),
+             "items per problem");
     cudaFree(b->d_tasks1d);
     b->d_tasks1d = nullptr;
     b->ntasks1d = (int)tasks.size();
@@ -276,6 +287,8 @@ BatchStageParams stage_params(const mc_batch* b, int part, int st, int dynamic, 
     bp.n_items = part == mc::kPart2d ? b->n2d : part == mc::kPart1d ? bundles : b->n2d + bundles;
     bp.dynamic = dynamic;
     bp.counter = counter;
+    bp.items_of = b->d_items_of;
+    bp.finished = b->d_finished + (size_t)st * b->n;
     return bp;
 }
 
@@ -298,7 +311,7 @@ mc_status enqueue_step(mc_batch* b, double* pool, cudaStream_t s) {
             MCB_CUDA(launch_stage(b, bp, mc::kPart1d, b->grid1d, s, nullptr), "batch stage");
         }
     }
-    batch_clock_kernel<<<cdiv(b->n, 256), 256, 0, s>>>(b->d_blocks, b->n, 0, b->d_counters);
+    batch_clock_kernel<<<cdiv(b->n, 256), 256, 0, s>>>(b->d_blocks, b->n, 0, b->d_counters, b->d_finished);
     MCB_CUDA(cudaGetLastError(), "batch clock");
     return MC_OK;
 }
@@ -321,7 +334,7 @@ mc_status init_clocks(mc_batch* b, double* pool, cudaStream_t s) {
              "clocks");
     batch_cfl_kernel<<<b->n, 256, 0, s>>>(b->d_params, b->d_offsets, pool);
     MCB_CUDA(cudaGetLastError(), "batch cfl");
-    batch_clock_kernel<<<cdiv(b->n, 256), 256, 0, s>>>(b->d_blocks, b->n, 1, b->d_counters);
+    batch_clock_kernel<<<cdiv(b->n, 256), 256, 0, s>>>(b->d_blocks, b->n, 1, b->d_counters, b->d_finished);
     MCB_CUDA(cudaGetLastError(), "batch clock");
     MCB_CUDA(cudaStreamSynchronize(s), "sync");  // blk must outlive the copy
     b->clocks_ready = true;
@@ -415,6 +428,8 @@ mc_status mc_batch_create(const mc_batch_problem* problems, int32_t n, const mc_
     alloc((void**)&b->d_stage, sizeof(StageParams) * 4 * (size_t)n);
     alloc((void**)&b->d_blocks, sizeof(DeviceBlock) * n);
     alloc((void**)&b->d_counters, sizeof(int) * kCounters);
+    alloc((void**)&b->d_finished, sizeof(int) * 4 * (size_t)n);
+    alloc((void**)&b->d_items_of, sizeof(int) * (size_t)n);
     if (e == cudaSuccess) {
         e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     }
@@ -463,11 +478,13 @@ mc_status mc_batch_create(const mc_batch_problem* problems, int32_t n, const mc_
         }
     }
     std::stable_sort(order2d.begin(), order2d.end(), [&](int a, int c) { return b->cells[a] > b->cells[c]; });
+    b->tiles_of.assign(n, 0);
     for (int i : order2d) {
         const StageParams& p = b->params[i];
         for (int by = 0; by < cdiv(p.ny, mc::kTile); ++by) {
             for (int bx = 0; bx < cdiv(p.nx, mc::kTile); ++bx) {
                 items.push_back({i, bx, by, 0});
+                b->tiles_of[i] += 1;
             }
         }
     }
@@ -486,6 +503,9 @@ mc_status mc_batch_create(const mc_batch_problem* problems, int32_t n, const mc_
     }
     if (e == cudaSuccess) {
         e = cudaMemset(b->d_counters, 0, sizeof(int) * kCounters);
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemset(b->d_finished, 0, sizeof(int) * 4 * (size_t)n);
     }
     if (e != cudaSuccess) {
         mc_batch_destroy(b);
@@ -528,6 +548,8 @@ mc_status mc_batch_destroy(mc_batch* b) {
     cudaFree(b->d_stage);
     cudaFree(b->d_blocks);
     cudaFree(b->d_counters);
+    cudaFree(b->d_finished);
+    cudaFree(b->d_items_of);
     cudaFree(b->d_items2d);
     cudaFree(b->d_tasks1d);
     if (b->ev_in) {
@@ -581,6 +603,7 @@ mc_status mc_batch_tune(mc_batch* b, double* pool, void* stream) {
         float tmin = 1e30f;
         for (int rep = 0; rep < 3; ++rep) {
             MCB_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(int) * kCounters, b->stream), "counters");
+            MCB_CUDA(cudaMemsetAsync(b->d_finished, 0, sizeof(int) * 4 * (size_t)b->n, b->stream), "counters");
             const BatchStageParams bp = stage_params(b, part, 0, dyn, b->d_counters);
             MCB_CUDA(cudaEventRecord(t0, b->stream), "event");
             MCB_CUDA(launch_stage(b, bp, part, grid, b->stream, nullptr), "tune launch");
@@ -670,6 +693,7 @@ mc_status mc_batch_tune(mc_batch* b, double* pool, void* stream) {
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     MCB_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(int) * kCounters, b->stream), "counters");
+    MCB_CUDA(cudaMemsetAsync(b->d_finished, 0, sizeof(int) * 4 * (size_t)b->n, b->stream), "counters");
     MCB_CUDA(cudaStreamSynchronize(b->stream), "sync");
     return build_tasks(b, b->segs);
 }

@@ -13,6 +13,15 @@
 // dynamically from an atomic counter. Every problem has its own
 // DeviceBlock: its dt, clock, CFL-minimum cell and status, so each problem
 // advances with its own dt.
+//
+// Ghost cells: the work items store only their own cells. Each finished
+// item is counted per problem (after a fence), and the CTA (2D) or warp
+// (1D) that finishes a problem's last item of the stage fills that
+// problem's ghost cells from the stored values (fill_ghosts). Nothing waits:
+// the last finisher does the work. The values and CFL bounds are those of
+// the single-problem kernels' per-cell scatter, without its divergence in
+// the tile body (the scatter in the tile body took a quarter of the batch's
+// time).
 #pragma once
 
 #include "stage_kernels.cuh"
@@ -37,6 +46,8 @@ struct BatchStageParams {
     int n_items;                // work items of this launch: the tiles, the 1D bundles or both
     int dynamic;
     int* counter;               // work counter of this launch (dynamic schedule)
+    const int* items_of;        // per problem: its work items in a stage (2D tiles or 1D tasks)
+    int* finished;              // per problem: its items of this stage finished so far
 };
 
 constexpr int kPart2d = 0;   // the launch over the 2D tiles
@@ -90,8 +101,22 @@ __device__ __forceinline__ void batch_tile(const BatchStageParams& bp, int item,
     if (!p.blk->done) {
         double dtmin = __longlong_as_double((long long)kInfBits);
         unsigned flags = 0;
-        tile2d<2, REC, LIM, RS, T, false, NT>(p, it.bx, it.by, 0, smem, dtmin, flags);
+        tile2d<2, REC, LIM, RS, T, false, NT, false, false, false>(p, it.bx, it.by, 0, smem, dtmin, flags);
         block_publish(dtmin, flags, p.last != 0, p.blk, red_d, red_u);
+        // the CTA that finishes the problem's last tile fills its ghost cells
+        __shared__ int s_last;
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_last = atomicAdd(&bp.finished[it.prob], 1) == bp.items_of[it.prob] - 1;
+        }
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            unsigned gflags = 0;
+            const double gmin = fill_ghosts<2, T>(p, threadIdx.x, NT, &gflags);
+            block_publish(gmin, gflags, p.last != 0, p.blk, red_d, red_u);
+        }
     }
 }
 
@@ -108,7 +133,18 @@ __device__ __forceinline__ void batch_bundle(const BatchStageParams& bp, int bun
             unsigned flags = 0;
             T* W = smem + (size_t)warp * 3 * seg1d_window<REC>();
             for (int s = 0; s < task.nseg; ++s) {
-                segment1d<REC, LIM, RS, T>(p, (task.s0 + s) * kTile, W, dtmin, flags);
+                segment1d<REC, LIM, RS, T, false, false>(p, (task.s0 + s) * kTile, W, dtmin, flags);
+            }
+            // the warp that finishes the problem's last task fills its ghosts
+            __threadfence();
+            __syncwarp();
+            int last = 0;
+            if (lane == 0) {
+                last = atomicAdd(&bp.finished[task.prob], 1) == bp.items_of[task.prob] - 1;
+            }
+            if (__shfl_sync(0xffffffffu, last, 0)) {
+                __threadfence();
+                dtmin = smin(fill_ghosts<1, T>(p, lane, 32, &flags), dtmin);
             }
             dtmin = warp_min(dtmin);
             flags = warp_or(flags);

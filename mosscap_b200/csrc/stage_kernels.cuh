@@ -221,6 +221,48 @@ __device__ __forceinline__ double scatter_ghosts(const StageParams& p, int i, in
     return dtmin;
 }
 
+// Every ghost cell of a 1D or 2D state, from the stored new values of the
+// interior cells next to a face: the cells whose scatter_ghosts has
+// targets, shared out over `count` threads starting at `first`. The values
+// are read through L2 (they were written by other CTAs, which fenced their
+// stores before the caller learned they were done). Returns the CFL minimum
+// over the ghosts (last stage) and ORs their flags into *flags: with each
+// cell's own store (write_own), the same values and bounds as write_cell.
+template <int NDIM, class T>
+__device__ double fill_ghosts(const StageParams& p, int first, int count, unsigned* flags) {
+    const int ng = p.ng, nx = p.nx, ny = NDIM > 1 ? p.ny : 1;
+    const long long vs = (long long)p.zc * p.yc * p.xc;
+    const int xc_near = nx < 2 * ng ? nx : 2 * ng;                  // interior columns next to an x face
+    const int yr_near = NDIM > 1 ? (ny < 2 * ng ? ny : 2 * ng) : 1; // interior rows next to a y face (1D: the one row)
+    const long long n_near_rows = NDIM > 1 ? (long long)yr_near * nx : 0;
+    const long long n_far = (long long)(ny - (NDIM > 1 ? yr_near : 0)) * xc_near;
+    double dtmin = __longlong_as_double(0x7ff0000000000000ll);
+    for (long long t = first; t < n_near_rows + n_far; t += count) {
+        int ii, jj;
+        if (t < n_near_rows) {
+            const int r = (int)(t / nx);
+            ii = (int)(t - (long long)r * nx);
+            jj = (r < ng || yr_near < 2 * ng) ? r : ny - yr_near + r;
+        } else {
+            const long long u = t - n_near_rows;
+            const int q = (int)(u / xc_near);
+            const int cc = (int)(u - (long long)q * xc_near);
+            jj = NDIM > 1 ? ng + q : 0;
+            ii = (cc < ng || xc_near < 2 * ng) ? cc : nx - xc_near + cc;
+        }
+        const int i = ng + ii;
+        const int j = NDIM > 1 ? ng + jj : 0;
+        const double* src = p.q_out + qidx(p, 0, 0, j, i);
+        double qn[kMaxVars];
+#pragma unroll
+        for (int v = 0; v < kMaxVars; ++v) {
+            qn[v] = v < p.nvar ? __ldcg(src + v * vs) : 0.0;
+        }
+        dtmin = smin(scatter_ghosts<NDIM, T>(p, i, j, 0, qn, p.last != 0, flags), dtmin);
+    }
+    return dtmin;
+}
+
 // Write the new value of interior cell (i, j, k) and every ghost it is the
 // source of; returns the CFL minimum over the written values (last stage) and
 // ORs their status flags into *flags.
@@ -451,7 +493,9 @@ __host__ __device__ constexpr int seg1d_window() {
     return kTile + 2 * halo_of<REC>();
 }
 
-template <int REC, int LIM, int RS, class T, bool SRC = false>
+// SCATTER false: only the cell itself is stored (the batched kernel fills a
+// problem's ghosts once all its cells are written: fill_ghosts).
+template <int REC, int LIM, int RS, class T, bool SRC = false, bool SCATTER = true>
 __device__ __forceinline__ void segment1d(const StageParams& p, int x0, T* W, double& dtmin, unsigned& flags) {
     constexpr int NDIM = 1;
     constexpr int nh = 3;
@@ -502,7 +546,11 @@ __device__ __forceinline__ void segment1d(const StageParams& p, int x0, T* W, do
                 qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qu, 0.0);
             }
         }
-        dtmin = smin(write_cell<NDIM, T>(p, i, 0, 0, qn, p.last != 0, &flags), dtmin);
+        if constexpr (SCATTER) {
+            dtmin = smin(write_cell<NDIM, T>(p, i, 0, 0, qn, p.last != 0, &flags), dtmin);
+        } else {
+            dtmin = smin(write_own<NDIM, T>(p, i, 0, 0, qn, p.last != 0, &flags), dtmin);
+        }
     }
 }
 
@@ -540,7 +588,7 @@ __global__ void __launch_bounds__(kThreads) stage1d_kernel(StageParams p) {
 // on mbar) instead of per-thread loads. Without TMA, smem holds W and then
 // the y divergences (smem_bytes).
 template <int NDIM, int REC, int LIM, int RS, class T, bool SRC = false, int NT = kThreads, bool TMA = false,
-          bool DEFER = false>
+          bool DEFER = false, bool SCATTER = true>
 __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int bz, T* smem, double& dtmin,
                                        unsigned& flags, const CUtensorMap* tmap = nullptr, uint64_t* mbar = nullptr) {
     constexpr int nh = 2 + NDIM;
@@ -731,7 +779,11 @@ __device__ __forceinline__ void tile2d(const StageParams& p, int bx, int by, int
                         qn[nh + t] = combine(p.combo, old ? p.q_old[id] : 0.0, p.q_in[id], qt, 0.0);
                     }
                 }
-                dtmin = smin(write_cell<NDIM, T>(p, i, j, 0, qn, p.last != 0, &flags), dtmin);
+                if constexpr (SCATTER) {
+                    dtmin = smin(write_cell<NDIM, T>(p, i, j, 0, qn, p.last != 0, &flags), dtmin);
+                } else {
+                    dtmin = smin(write_own<NDIM, T>(p, i, j, 0, qn, p.last != 0, &flags), dtmin);
+                }
             }
         }
         __syncthreads();
