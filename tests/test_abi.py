@@ -60,8 +60,9 @@ def test_enum_values_are_reference_ordinals():
 
 
 def test_slab_and_batch_form_entry_points_reject_bad_arguments():
-    """Argument checks of the adjoint's slab entry points and the batch's
-    launch-form switch, which fail before any device call."""
+    """Argument checks of the adjoint's slab entry points, the batch's
+    launch-form switch, the host-resident step and the slab overlap switch,
+    which fail before any device call."""
     lib = capi.load()
     INVALID = 1  # MC_ERR_INVALID_ARGUMENT
     assert capi.STATUS_NAMES[INVALID] == "MC_ERR_INVALID_ARGUMENT"
@@ -70,6 +71,9 @@ def test_slab_and_batch_form_entry_points_reject_bad_arguments():
     assert lib.mc_adjoint_set_slab_hook(None, hook, None, 0, 1) == INVALID
     assert lib.mc_adjoint_set_slab_decomposition(None, uid, 0, 1) == INVALID
     assert lib.mc_batch_set_stage_launches(None, 1) == INVALID
+    dt = ctypes.c_double()
+    assert lib.mc_step_host(None, None, None, None, ctypes.byref(dt), None) == INVALID
+    assert lib.mc_set_slab_overlap(None, 1) == INVALID
     n = ctypes.c_int32()
     assert lib.mc_batch_stage_launches(None, ctypes.byref(n)) == INVALID
     # the hook operation codes are the header's
