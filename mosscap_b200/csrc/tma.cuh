@@ -1,9 +1,9 @@
 // Tensor-memory-accelerator (TMA) tile loads of the conserved state.
 //
 // The tiled stage kernels stage the haloed tile of Q that a CTA converts to
-// primitives with one cp.async.bulk.tensor copy into shared memory (no
-// multicast: every CTA loads its own tile from this GPU's memory), completed
-// on an mbarrier, instead of one global load per thread, cell and variable.
+// primitives with one cp.async.bulk.tensor copy into shared memory (every
+// CTA loads its own tile, from this GPU's memory only), completed on an
+// mbarrier, instead of one global load per thread, cell and variable.
 //
 // Device side: mbarrier set-up, the tensor copy and a bounded wait. Host
 // side (tma_map_for): the tensor map of a state array, encoded with the
