@@ -54,7 +54,7 @@ struct mc_ctx {
     // mc_step_host: copy streams and events of its pipeline (created on first use)
     cudaStream_t hs_in = nullptr, hs_out = nullptr;
     cudaEvent_t hs_fork = nullptr, hs_join = nullptr;
-    cudaEvent_t hs_ev_in[8] = {}, hs_ev_out[8] = {};
+    cudaEvent_t hs_ev_in[16] = {}, hs_ev_out[16] = {};
     int gravity = 0;              // mc_set_gravity
     double grav[3] = {0.0, 0.0, 0.0};
     // non-ideal EOS (mc_set_eos)
@@ -390,7 +390,7 @@ mc_status enqueue_step_overlapped(mc_ctx* c, double* Q, double dt, const double*
 
 // ---- mc_step_host ------------------------------------------------------------
 
-constexpr int kHostBands = 8;  // bands of tile rows of the pipelined host step
+constexpr int kHostBands = 16;  // bands of tile rows of the pipelined host step (16: 1.3 % faster than 8 on KH 2048^2)
 
 // Whether mc_step_host overlaps its copies with the step (2D, ideal EOS, no
 // hooks or slab exchange, at least two tile rows).
