@@ -56,6 +56,31 @@ def test_batch_matches_oracle_per_problem(gpu_lib, oracle_port, rs):
     assert checked >= len(probs) - 4
 
 
+@pytest.mark.parametrize("stepper", ["ssprk3", "ssprk4"])
+def test_batch_other_steppers_match_oracle(gpu_lib, oracle_port, stepper):
+    """Three- and four-stage steppers: every stage's ghost cells are filled
+    by each problem's last finishing tile or task of that stage (one count
+    per stage and problem), bit-identical to the oracle per problem."""
+    from mosscap_b200 import capi
+    from mosscap_b200.hydro import BatchSim
+    probs = [p.with_scheme(time_stepper=stepper) for p in _small_batch("hllc", seed=17)]
+    steps = 6
+    b = BatchSim(probs)
+    b.fill_bcs()
+    b.advance(steps)
+    _, nsteps, status = b.clocks()
+    checked = 0
+    for k, p in enumerate(probs):
+        ref = _oracle_run(oracle_port, p, steps)
+        if np.isfinite(ref).all():
+            assert nsteps[k] == steps, k
+            assert np.array_equal(_bits(b.get_Q(k)), _bits(ref)), f"problem {k} ({p.name}) differs"
+            checked += 1
+        else:
+            assert status[k] & (capi.FLAG_NONFINITE | capi.FLAG_NEG_PRESSURE | capi.FLAG_NEG_DENSITY), k
+    assert checked >= len(probs) - 4
+
+
 def test_batch_schedule_independent(gpu_lib):
     """Tuned and default schedules (static / dynamic, grid sizes, 1D task
     lengths) give bit-identical states and clocks."""

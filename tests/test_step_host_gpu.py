@@ -42,6 +42,12 @@ def _problem(case):
                          bc=("zerograd", "wall", "periodic", "periodic", "zerograd", "zerograd"),
                          reconstruction="ppm", slope_limiter="monotonizedcentral", riemann_solver="hll",
                          time_stepper="ssprk4", gamma=1.4, max_cfl=0.5, Q=q), "fp32"
+    if case == "weno5z_hllc_ssprk3_fp32_gravity":
+        q = P.random_state(2, 72, 97, ng=3, seed=21)
+        return P.Problem("host_fp32_gravity", 2, 72, 97, ng=3, dx=1.0 / 97,
+                         bc=("periodic", "periodic", "wall", "zerograd", "zerograd", "zerograd"),
+                         reconstruction="weno5z", riemann_solver="hllc", time_stepper="ssprk3", gamma=1.4,
+                         max_cfl=0.4, gravity=(0.0, -2.0, 0.0), Q=q), "fp32"
     if case == "serial_2d_few_rows":
         q = P.random_state(2, 50, 24, ng=3, seed=3)
         return P.Problem("host_small", 2, 50, 24, ng=3, dx=1.0 / 50, bc=("zerograd",) * 6,
@@ -73,7 +79,8 @@ def _serial(p, precision):
 
 @pytest.mark.parametrize("pinned", [True, False])
 @pytest.mark.parametrize("case", ["weno5z_hllc_ssprk3_periodic", "muscl_rusanov_rk2_gravity_tracers", "ppm_hll_ssprk4_fp32",
-                                  "serial_2d_few_rows", "serial_sod_1d", "serial_3d"])
+                                  "weno5z_hllc_ssprk3_fp32_gravity", "serial_2d_few_rows", "serial_sod_1d",
+                                  "serial_3d"])
 def test_step_host_matches_serial_calls(gpu_lib, case, pinned):
     from mosscap_b200.hydro import HydroSim
     if not pinned and case != "weno5z_hllc_ssprk3_periodic":
