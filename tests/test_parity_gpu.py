@@ -447,3 +447,23 @@ def test_slab_overlap_single_rank(gpu_lib, oracle_port, ny, st, rec, rs, gravity
             assert n == steps * nst and ms > 0.0, (what, n, ms)
             assert s.sim.status() == 0
             s.sim.close()
+
+
+def test_slab_overlap_fp32_form_matches_serial_exchange(gpu_lib):
+    """The FP32 compute form through the overlapped slab step (one rank,
+    the library's NCCL path): bit-identical to the same slab with the
+    overlap off, in the device-driven loop."""
+    from mosscap_b200 import capi
+    from mosscap_b200.distributed import SlabSim
+    p = P.kelvin_helmholtz_2d(128, seed=9).with_scheme(max_time=1e30, output_delta=1e30)
+    runs = []
+    for overlap in (1, 0):
+        s = SlabSim(p, rank=0, world=1, precision="fp32", transport="library")
+        capi.check(s.sim.lib.mc_set_slab_overlap(s.sim.ctx, overlap), "mc_set_slab_overlap")
+        s.fill_bcs()
+        dts = np.array(s.advance(10))
+        runs.append((dts, s.sim.get_Q()))
+        assert s.sim.status() == 0
+        s.sim.close()
+    _assert_same(runs[0][0], runs[1][0], "dt")
+    _assert_same(runs[0][1], runs[1][1], "state")
